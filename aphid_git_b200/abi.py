@@ -1,0 +1,241 @@
+"""ctypes binding of the C ABI (include/aphid_gpu.h).
+
+The names mirror the reference's routines (src/aphid.f90, src/aphid_qmr.f90):
+``inprod`` (inprod_x/y/z/p), ``gen_k2`` (gen_k2_*grid), ``gen_diag``,
+``qmr`` and ``gen_fields``.  Vectors are numpy complex128 arrays in the
+reference's unknown order [Ax | Ay | Az | Phi], each block Fortran-ordered.
+
+There is no CPU fallback: if libaphid_gpu.so is missing or no sm_100 device
+is present, every entry point raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+APHID_OK = 0
+STATUS = {0: "converged", 1: "maxit", 2: "breakdown", 3: "nonfinite"}
+ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory",
+          -4: "call order", -5: "no sm_100 device"}
+PREC_FP64, PREC_MIXED = 0, 1
+
+
+class AphidError(RuntimeError):
+    pass
+
+
+class Opts(C.Structure):
+    _fields_ = [("device", C.c_int), ("stream", C.c_void_p), ("graph_iters", C.c_int),
+                ("verbose", C.c_int)]
+
+
+class Info(C.Structure):
+    _fields_ = [("status", C.c_int), ("iters", C.c_int), ("inner_iters", C.c_int),
+                ("outer_iters", C.c_int), ("rhs_norm", C.c_double), ("recur_resid", C.c_double),
+                ("true_rel_resid", C.c_double), ("seconds", C.c_double),
+                ("kernel_launches", C.c_longlong)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["status_name"] = STATUS.get(self.status, str(self.status))
+        return d
+
+
+_lib = None
+_Z = C.c_void_p
+
+
+def library_path():
+    return _build.LIB
+
+
+def load():
+    """Load libaphid_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise AphidError("libaphid_gpu.so not built: run `python -m aphid_git_b200.build`")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    L.aphid_gpu_create.argtypes = [C.POINTER(P), C.POINTER(Opts)]
+    L.aphid_gpu_destroy.argtypes = [P]
+    L.aphid_gpu_last_error.argtypes = [P]
+    L.aphid_gpu_last_error.restype = C.c_char_p
+    L.aphid_gpu_set_mesh.argtypes = [P, C.c_int, C.c_int, C.c_int] + [P] * 6
+    L.aphid_gpu_inprod.argtypes = [P] + [_Z] * 12
+    L.aphid_gpu_gen_k2.argtypes = [P, _Z, C.c_double] + [_Z] * 4
+    L.aphid_gpu_gen_diag.argtypes = [P] + [_Z] * 8
+    L.aphid_gpu_qmr.argtypes = [P] + [_Z] * 16 + [C.c_double, C.c_int, P, C.c_int,
+                                                   C.POINTER(Info)]
+    L.aphid_gpu_fields.argtypes = [P, C.c_double] + [_Z] * 10
+    L.aphid_gpu_qmr_load.argtypes = [P] + [_Z] * 12
+    L.aphid_gpu_qmr_run.argtypes = [P, C.c_double, C.c_int, C.c_int, P, C.c_int, C.POINTER(Info)]
+    L.aphid_gpu_qmr_fetch.argtypes = [P] + [_Z] * 4
+    L.aphid_gpu_inprod_dev.argtypes = [P, P, P, P, P]
+    _lib = L
+    return L
+
+
+def nunk(nx, ny, nz):
+    return (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1) + nx * ny * nz
+
+
+def block_offsets(nx, ny, nz):
+    ox = 0
+    oy = (nx - 1) * ny * nz
+    oz = oy + nx * (ny - 1) * nz
+    op = oz + nx * ny * (nz - 1)
+    return [ox, oy, oz, op, op + nx * ny * nz]
+
+
+def _c128(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    if n is not None and a.size != n:
+        raise ValueError("expected %d complex values, got %d" % (n, a.size))
+    return a
+
+
+class Solver:
+    """One GPU context (one per host thread), bound to a mesh."""
+
+    def __init__(self, device=0, stream=None, graph_iters=0, verbose=False):
+        self.lib = load()
+        self._h = C.c_void_p()
+        o = Opts(device, stream or 0, graph_iters, int(verbose))
+        rc = self.lib.aphid_gpu_create(C.byref(self._h), C.byref(o))
+        if rc != APHID_OK:
+            raise AphidError("aphid_gpu_create failed: %s" % ERRORS.get(rc, rc))
+        self.dims = None
+
+    def close(self):
+        if self._h:
+            self.lib.aphid_gpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != APHID_OK:
+            msg = self.lib.aphid_gpu_last_error(self._h).decode()
+            raise AphidError("%s: %s (%s)" % (what, ERRORS.get(rc, rc), msg))
+
+    # ------------------------------------------------------------- mesh
+    def set_mesh(self, dx, dy, dz, dxc, dyc, dzc):
+        """dx(0:n), dxc(1:n) per axis (the reference's module mesh arrays)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (dx, dy, dz, dxc, dyc, dzc)]
+        nx, ny, nz = len(arrs[3]), len(arrs[4]), len(arrs[5])
+        if [len(a) for a in arrs[:3]] != [nx + 1, ny + 1, nz + 1]:
+            raise ValueError("dx must have n+1 values and dxc n values per axis")
+        self._keep = arrs
+        self._check(self.lib.aphid_gpu_set_mesh(self._h, nx, ny, nz,
+                                                *[a.ctypes.data for a in arrs]), "set_mesh")
+        self.dims = (nx, ny, nz)
+        self.n = nunk(nx, ny, nz)
+        self.off = block_offsets(nx, ny, nz)
+
+    def set_nodes(self, xn, yn, zn):
+        from .model import spacings
+        (dx, dxc), (dy, dyc), (dz, dzc) = spacings(xn), spacings(yn), spacings(zn)
+        self.set_mesh(dx, dy, dz, dxc, dyc, dzc)
+
+    def _blocks(self, v):
+        b = v.ctypes.data
+        return [b + 16 * o for o in self.off[:4]]
+
+    # --------------------------------------------------------- operators
+    def inprod(self, k2, x):
+        """y = K x (inprod_x, inprod_y, inprod_z, inprod_p)."""
+        k2, x = _c128(k2, self.n), _c128(x, self.n)
+        y = np.empty(self.n, np.complex128)
+        self._check(self.lib.aphid_gpu_inprod(self._h, *self._blocks(k2), *self._blocks(x),
+                                              *self._blocks(y)), "inprod")
+        return y
+
+    def gen_k2(self, sig, omega):
+        nx, ny, nz = self.dims
+        sig = _c128(sig, (nx - 1) * (ny - 1) * (nz - 1))
+        k2 = np.empty(self.n, np.complex128)
+        self._check(self.lib.aphid_gpu_gen_k2(self._h, sig.ctypes.data, float(omega),
+                                              *self._blocks(k2)), "gen_k2")
+        return k2
+
+    def gen_diag(self, k2):
+        k2 = _c128(k2, self.n)
+        d = np.empty(self.n, np.complex128)
+        self._check(self.lib.aphid_gpu_gen_diag(self._h, *self._blocks(k2), *self._blocks(d)),
+                    "gen_diag")
+        return d
+
+    def qmr(self, k2, diag, b, target, max_it, x0=None, hist=True):
+        """Solve K x = b like `call qmr`.  Returns (x, info dict, hist array)."""
+        k2, diag = _c128(k2, self.n), _c128(diag, self.n)
+        x = _c128(b, self.n).copy()
+        x0a = _c128(x0, self.n) if x0 is not None else None  # keep alive across the call
+        x0p = self._blocks(x0a) if x0a is not None else [None] * 4
+        cap = max(1, max_it) if hist else 0
+        h = np.zeros(max(cap, 1))
+        info = Info()
+        self._check(self.lib.aphid_gpu_qmr(self._h, *self._blocks(k2), *self._blocks(diag),
+                                           *self._blocks(x), *x0p, float(target), int(max_it),
+                                           h.ctypes.data if hist else None, cap,
+                                           C.byref(info)), "qmr")
+        d = info.as_dict()
+        nh = min(d["inner_iters"], cap)
+        return x, d, h[:nh]
+
+    def qmr_load(self, k2, diag, b):
+        """Make k2, diag and b resident on the device (aphid_gpu_qmr_load)."""
+        self._res = [_c128(k2, self.n), _c128(diag, self.n), _c128(b, self.n)]
+        self._check(self.lib.aphid_gpu_qmr_load(self._h, *self._blocks(self._res[0]),
+                                                *self._blocks(self._res[1]),
+                                                *self._blocks(self._res[2])), "qmr_load")
+
+    def qmr_run(self, target, max_it, use_previous_x=False, hist=False):
+        """Solve the resident problem; the solution stays on the device."""
+        cap = max(1, max_it) if hist else 0
+        h = np.zeros(max(cap, 1))
+        info = Info()
+        self._check(self.lib.aphid_gpu_qmr_run(self._h, float(target), int(max_it),
+                                               int(bool(use_previous_x)),
+                                               h.ctypes.data if hist else None, cap,
+                                               C.byref(info)), "qmr_run")
+        d = info.as_dict()
+        return d, h[:min(d["inner_iters"], cap)]
+
+    def qmr_fetch(self):
+        x = np.empty(self.n, np.complex128)
+        self._check(self.lib.aphid_gpu_qmr_fetch(self._h, *self._blocks(x)), "qmr_fetch")
+        return x
+
+    def inprod_dev(self, d_k2, d_in, d_out, d_eps=None):
+        """y = K x on device pointers (concatenated complex128 vectors);
+        asynchronous on the context's stream."""
+        self._check(self.lib.aphid_gpu_inprod_dev(self._h, d_k2, d_in, d_out, d_eps),
+                    "inprod_dev")
+
+    def gen_fields(self, omega, sol):
+        """(B, E): B = curl A on faces [Bx|By|Bz], E on edges [Ex|Ey|Ez]."""
+        nx, ny, nz = self.dims
+        sol = _c128(sol, self.n)
+        nb = [nx * (ny - 1) * (nz - 1), (nx - 1) * ny * (nz - 1), (nx - 1) * (ny - 1) * nz]
+        B = np.empty(sum(nb), np.complex128)
+        E = np.empty(self.off[3], np.complex128)
+        bp = [B.ctypes.data, B.ctypes.data + 16 * nb[0], B.ctypes.data + 16 * (nb[0] + nb[1])]
+        ep = [E.ctypes.data + 16 * o for o in self.off[:3]]
+        self._check(self.lib.aphid_gpu_fields(self._h, float(omega), *self._blocks(sol), *bp,
+                                              *ep), "gen_fields")
+        return B, E

@@ -1,0 +1,603 @@
+// aphid_gpu.cu -- C ABI (include/aphid_gpu.h) over the sm_100a kernels.
+//
+// Host orchestration only: argument checks, host<->device copies at the
+// reference's array boundaries, launch geometry, and the CUDA-graph replay of
+// the QMR iteration.  All arithmetic of the solve runs on the GPU; there is no
+// CPU fallback (a missing or unsupported device is an error).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/aphid_gpu.h"
+#include "aphid_qmr64.cuh"
+
+using namespace aphid;
+
+struct aphid_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int graph_iters = 16;
+  int verbose = 0;
+  std::string err;
+
+  // mesh
+  bool has_mesh = false;
+  int nx = 0, ny = 0, nz = 0;
+  long long n = 0;
+  double *d_tab = nullptr;
+  GridDev g{};
+  Tiles tiles{};
+  int sblk = 0;  // blocks of the streaming kernels
+
+  // complex128 work space: k2 inv b x r s p d v q
+  double2 *w64 = nullptr;
+  Scal64 *d_sc = nullptr;
+  double *d_part = nullptr;
+  unsigned *d_cnt = nullptr;
+  double *d_hist = nullptr;
+  int hist_alloc = 0;
+  double *d_out = nullptr;
+  int *h_done = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // captured QMR iteration
+  cudaGraphExec_t gexec = nullptr;
+  const void *gkey = nullptr;
+
+  // resident problem state (aphid_gpu_qmr_load / _run / _fetch)
+  bool loaded = false;     // k2, diag and b are on the device
+  bool inv_ready = false;  // W_INV holds 1/diag (else diag)
+};
+
+namespace {
+
+enum { W_K2, W_INV, W_B, W_X, W_R, W_S, W_P, W_D, W_V, W_Q, W_COUNT };
+
+int fail(aphid_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(aphid_ctx *c, cudaError_t e, const char *what) {
+  return fail(c, APHID_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+double2 *wv(aphid_ctx *ctx, int which) { return ctx->w64 + (size_t)which * ctx->n; }
+
+// Coefficient tables of one axis (gen_inprod_*_coefs, src/aphid.f90:750-1185)
+void axis_tables(int n, const double *d, const double *dc, std::vector<double> &out) {
+  // layout: d[n+1] dc[n] e2[n-1] e3[n-1] n4[n] n5[n]
+  out.clear();
+  out.insert(out.end(), d, d + n + 1);
+  out.insert(out.end(), dc, dc + n);
+  for (int e = 0; e < n - 1; e++) out.push_back(mask_hi(e + 1, n - 1) / dc[e + 1] / d[e + 1]);
+  for (int e = 0; e < n - 1; e++) out.push_back(mask_lo(e + 1, n) / dc[e] / d[e + 1]);
+  for (int m = 0; m < n; m++) out.push_back(mask_hi(m + 1, n) / d[m + 1] / dc[m]);
+  for (int m = 0; m < n; m++) out.push_back(mask_lo(m + 1, n) / d[m] / dc[m]);
+}
+
+void release_work(aphid_ctx *ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  ctx->gexec = nullptr;
+  ctx->gkey = nullptr;
+  cudaFree(ctx->w64);
+  cudaFree(ctx->d_sc);
+  cudaFree(ctx->d_part);
+  cudaFree(ctx->d_cnt);
+  cudaFree(ctx->d_hist);
+  cudaFree(ctx->d_out);
+  ctx->w64 = nullptr;
+  ctx->d_sc = nullptr;
+  ctx->d_part = nullptr;
+  ctx->d_cnt = nullptr;
+  ctx->d_hist = nullptr;
+  ctx->d_out = nullptr;
+  ctx->hist_alloc = 0;
+}
+
+int ensure_work(aphid_ctx *ctx) {
+  if (ctx->w64) return APHID_OK;
+  size_t bytes = (size_t)W_COUNT * ctx->n * sizeof(double2);
+  cudaError_t e = cudaMalloc(&ctx->w64, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->w64 = nullptr;
+    return fail(ctx, APHID_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  const long long slots = std::max<long long>(ctx->sblk, ctx->tiles.count());
+  CK(cudaMalloc(&ctx->d_sc, sizeof(Scal64)));
+  CK(cudaMalloc(&ctx->d_part, (size_t)slots * 3 * sizeof(double)));
+  CK(cudaMalloc(&ctx->d_cnt, 16 * sizeof(unsigned)));
+  CK(cudaMemset(ctx->d_cnt, 0, 16 * sizeof(unsigned)));
+  CK(cudaMalloc(&ctx->d_out, 8 * sizeof(double)));
+  return APHID_OK;
+}
+
+int upload4(aphid_ctx *ctx, double2 *dst, const aphid_z *a, const aphid_z *b, const aphid_z *c,
+            const aphid_z *d) {
+  const aphid_z *src[4] = {a, b, c, d};
+  const long long off[5] = {ctx->g.ox, ctx->g.oy, ctx->g.oz, ctx->g.op, ctx->n};
+  for (int q = 0; q < 4; q++)
+    CK(cudaMemcpyAsync(dst + off[q], src[q], (size_t)(off[q + 1] - off[q]) * sizeof(double2),
+                       cudaMemcpyHostToDevice, ctx->stream));
+  return APHID_OK;
+}
+
+int download4(aphid_ctx *ctx, const double2 *src, aphid_z *a, aphid_z *b, aphid_z *c, aphid_z *d) {
+  aphid_z *dst[4] = {a, b, c, d};
+  const long long off[5] = {ctx->g.ox, ctx->g.oy, ctx->g.oz, ctx->g.op, ctx->n};
+  for (int q = 0; q < 4; q++)
+    CK(cudaMemcpyAsync(dst[q], src + off[q], (size_t)(off[q + 1] - off[q]) * sizeof(double2),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  return APHID_OK;
+}
+
+bool all4(const void *a, const void *b, const void *c, const void *d) { return a && b && c && d; }
+
+int check_ready(aphid_ctx *ctx) {
+  if (!ctx) return APHID_ERR_BADARG;
+  if (!ctx->has_mesh) return fail(ctx, APHID_ERR_STATE, "aphid_gpu_set_mesh has not been called");
+  CK(cudaSetDevice(ctx->device));
+  return APHID_OK;
+}
+
+dim3 node_grid(const aphid_ctx *ctx) {
+  return dim3((unsigned)((ctx->nx + 127) / 128), (unsigned)ctx->ny, (unsigned)ctx->nz);
+}
+
+void launch_apply(aphid_ctx *ctx, const double2 *k2, const double2 *in, double2 *out) {
+  k_apply64<kApplyPlain><<<(unsigned)ctx->tiles.count(), kOpThreads, 0, ctx->stream>>>(
+      ctx->g, ctx->tiles, k2, in, out, nullptr, nullptr, nullptr, nullptr);
+}
+
+// One QMR iteration (src/aphid_qmr.f90:297-390) as four launches.
+void launch_iteration(aphid_ctx *ctx) {
+  const long long n = ctx->n;
+  const int sb = ctx->sblk;
+  double2 *inv = wv(ctx, W_INV), *x = wv(ctx, W_X), *r = wv(ctx, W_R), *s = wv(ctx, W_S);
+  double2 *p = wv(ctx, W_P), *d = wv(ctx, W_D), *v = wv(ctx, W_V), *q = wv(ctx, W_Q);
+  k_pupd64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, v, inv, p, ctx->d_sc);
+  k_apply64<kApplyQmr><<<(unsigned)ctx->tiles.count(), kOpThreads, 0, ctx->stream>>>(
+      ctx->g, ctx->tiles, wv(ctx, W_K2), p, q, ctx->d_sc, nullptr, ctx->d_part, ctx->d_cnt + 1);
+  k_rho64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, q, v, ctx->d_sc, ctx->d_part, ctx->d_cnt + 2);
+  k_upd64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, p, q, inv, d, x, s, r, v, ctx->d_sc, ctx->d_hist,
+                                                  ctx->d_part, ctx->d_cnt + 3);
+}
+
+int build_graph(aphid_ctx *ctx) {
+  if (ctx->gexec && ctx->gkey == (const void *)ctx->d_hist) return APHID_OK;
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  ctx->gexec = nullptr;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  for (int it = 0; it < ctx->graph_iters; it++) launch_iteration(ctx);
+  CK(cudaStreamEndCapture(ctx->stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+  ctx->gkey = (const void *)ctx->d_hist;
+  return APHID_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *aphid_gpu_last_error(const aphid_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int aphid_gpu_create(aphid_ctx **out, const aphid_opts *opts) {
+  if (!out) return APHID_ERR_BADARG;
+  *out = nullptr;
+  aphid_ctx *ctx = new aphid_ctx();
+  if (opts) {
+    ctx->device = opts->device;
+    ctx->stream = (cudaStream_t)opts->stream;
+    if (opts->graph_iters > 0) ctx->graph_iters = std::min(opts->graph_iters, 256);
+    ctx->verbose = opts->verbose;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev <= ctx->device || ctx->device < 0) {
+    cudaGetLastError();
+    delete ctx;
+    return APHID_ERR_NODEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess || prop.major != 10) {
+    delete ctx;
+    return APHID_ERR_NODEVICE;  // kernels are built for sm_100a only
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) {
+    delete ctx;
+    return APHID_ERR_NODEVICE;
+  }
+  if (!ctx->stream) {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return APHID_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+  }
+  if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_done, sizeof(int)) != cudaSuccess) {
+    delete ctx;
+    return APHID_ERR_CUDA;
+  }
+  *out = ctx;
+  return APHID_OK;
+}
+
+int aphid_gpu_destroy(aphid_ctx *ctx) {
+  if (!ctx) return APHID_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  release_work(ctx);
+  cudaFree(ctx->d_tab);
+  if (ctx->h_done) cudaFreeHost(ctx->h_done);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return APHID_OK;
+}
+
+int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz, const double *dx, const double *dy,
+                       const double *dz, const double *dxc, const double *dyc, const double *dzc) {
+  if (!ctx) return APHID_ERR_BADARG;
+  if (nx < 3 || ny < 3 || nz < 3) return fail(ctx, APHID_ERR_BADARG, "need at least 3 nodes per axis");
+  if (!dx || !dy || !dz || !dxc || !dyc || !dzc) return fail(ctx, APHID_ERR_BADARG, "null spacing array");
+  const long long n = (long long)(nx - 1) * ny * nz + (long long)nx * (ny - 1) * nz +
+                      (long long)nx * ny * (nz - 1) + (long long)nx * ny * nz;
+  const int dims[3] = {nx, ny, nz};
+  const double *ds[3] = {dx, dy, dz}, *dcs[3] = {dxc, dyc, dzc};
+  for (int a = 0; a < 3; a++) {
+    for (int m = 0; m <= dims[a]; m++)
+      if (!(ds[a][m] > 0.0) || !std::isfinite(ds[a][m]))
+        return fail(ctx, APHID_ERR_BADARG, "non-positive or non-finite node spacing");
+    for (int m = 0; m < dims[a]; m++)
+      if (!(dcs[a][m] > 0.0) || !std::isfinite(dcs[a][m]))
+        return fail(ctx, APHID_ERR_BADARG, "non-positive or non-finite dual spacing");
+  }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  release_work(ctx);
+  cudaFree(ctx->d_tab);
+  ctx->d_tab = nullptr;
+  ctx->has_mesh = false;
+
+  std::vector<double> all, one;
+  size_t offs[3];
+  for (int a = 0; a < 3; a++) {
+    axis_tables(dims[a], ds[a], dcs[a], one);
+    offs[a] = all.size();
+    all.insert(all.end(), one.begin(), one.end());
+  }
+  CK(cudaMalloc(&ctx->d_tab, all.size() * sizeof(double)));
+  CK(cudaMemcpy(ctx->d_tab, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+  GridDev g{};
+  for (int a = 0; a < 3; a++) {
+    const int m = dims[a];
+    const double *b = ctx->d_tab + offs[a];
+    g.ax[a].n = m;
+    g.ax[a].d = b;
+    g.ax[a].dc = b + (m + 1);
+    g.ax[a].e2 = b + (m + 1) + m;
+    g.ax[a].e3 = b + (m + 1) + m + (m - 1);
+    g.ax[a].n4 = b + (m + 1) + m + 2 * (m - 1);
+    g.ax[a].n5 = b + (m + 1) + m + 2 * (m - 1) + m;
+  }
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = nz;
+  g.ox = 0;
+  g.oy = (long long)(nx - 1) * ny * nz;
+  g.oz = g.oy + (long long)nx * (ny - 1) * nz;
+  g.op = g.oz + (long long)nx * ny * (nz - 1);
+  g.n = n;
+  ctx->g = g;
+  ctx->nx = nx;
+  ctx->ny = ny;
+  ctx->nz = nz;
+  ctx->n = n;
+  Tiles t;
+  t.ti = (nx + kTileI - 1) / kTileI;
+  t.tj = (ny + kTileJ - 1) / kTileJ;
+  const long long cols = (long long)t.ti * t.tj;
+  t.kz = (int)std::min<long long>(32, std::max<long long>(1, cols * nz / (148 * 8)));
+  t.tk = (nz + t.kz - 1) / t.kz;
+  ctx->tiles = t;
+  ctx->sblk = (int)std::max<long long>(1, std::min<long long>((n + kStreamThreads - 1) / kStreamThreads, 148 * 8));
+  ctx->has_mesh = true;
+  return APHID_OK;
+}
+
+int aphid_gpu_inprod(aphid_ctx *ctx, const aphid_z *k2_x, const aphid_z *k2_y, const aphid_z *k2_z,
+                     const aphid_z *k2_p, const aphid_z *in_x, const aphid_z *in_y,
+                     const aphid_z *in_z, const aphid_z *in_p, aphid_z *out_x, aphid_z *out_y,
+                     aphid_z *out_z, aphid_z *out_p) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!all4(k2_x, k2_y, k2_z, k2_p) || !all4(in_x, in_y, in_z, in_p) ||
+      !all4(out_x, out_y, out_z, out_p))
+    return fail(ctx, APHID_ERR_BADARG, "null array");
+  if ((rc = ensure_work(ctx))) return rc;
+  ctx->loaded = false;  // the work space is reused below
+  double2 *k2 = wv(ctx, W_K2), *in = wv(ctx, W_P), *out = wv(ctx, W_Q);
+  if ((rc = upload4(ctx, k2, k2_x, k2_y, k2_z, k2_p))) return rc;
+  if ((rc = upload4(ctx, in, in_x, in_y, in_z, in_p))) return rc;
+  launch_apply(ctx, k2, in, out);
+  CK(cudaGetLastError());
+  if ((rc = download4(ctx, out, out_x, out_y, out_z, out_p))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+int aphid_gpu_gen_k2(aphid_ctx *ctx, const aphid_z *sig, double omega, aphid_z *k2_x, aphid_z *k2_y,
+                     aphid_z *k2_z, aphid_z *k2_p) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!sig || !all4(k2_x, k2_y, k2_z, k2_p)) return fail(ctx, APHID_ERR_BADARG, "null array");
+  if (!std::isfinite(omega)) return fail(ctx, APHID_ERR_BADARG, "non-finite omega");
+  if ((rc = ensure_work(ctx))) return rc;
+  ctx->loaded = false;  // the work space is reused below
+  const long long ncell = (long long)(ctx->nx - 1) * (ctx->ny - 1) * (ctx->nz - 1);
+  double2 *dsig = wv(ctx, W_P), *k2 = wv(ctx, W_K2);  // ncell < n
+  CK(cudaMemcpyAsync(dsig, sig, ncell * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  k_gen_k2<<<node_grid(ctx), 128, 0, ctx->stream>>>(ctx->g, dsig, omega, k2);
+  CK(cudaGetLastError());
+  if ((rc = download4(ctx, k2, k2_x, k2_y, k2_z, k2_p))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+int aphid_gpu_gen_diag(aphid_ctx *ctx, const aphid_z *k2_x, const aphid_z *k2_y, const aphid_z *k2_z,
+                       const aphid_z *k2_p, aphid_z *diag_x, aphid_z *diag_y, aphid_z *diag_z,
+                       aphid_z *diag_p) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!all4(k2_x, k2_y, k2_z, k2_p) || !all4(diag_x, diag_y, diag_z, diag_p))
+    return fail(ctx, APHID_ERR_BADARG, "null array");
+  if ((rc = ensure_work(ctx))) return rc;
+  ctx->loaded = false;  // the work space is reused below
+  double2 *k2 = wv(ctx, W_K2), *dg = wv(ctx, W_Q);
+  if ((rc = upload4(ctx, k2, k2_x, k2_y, k2_z, k2_p))) return rc;
+  k_gen_diag<<<node_grid(ctx), 128, 0, ctx->stream>>>(ctx->g, k2, dg);
+  CK(cudaGetLastError());
+  if ((rc = download4(ctx, dg, diag_x, diag_y, diag_z, diag_p))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+namespace {
+
+int qmr_load(aphid_ctx *ctx, const aphid_z *k2_x, const aphid_z *k2_y, const aphid_z *k2_z,
+             const aphid_z *k2_p, const aphid_z *diag_x, const aphid_z *diag_y,
+             const aphid_z *diag_z, const aphid_z *diag_p, const aphid_z *rhs_x,
+             const aphid_z *rhs_y, const aphid_z *rhs_z, const aphid_z *rhs_p) {
+  if (!all4(k2_x, k2_y, k2_z, k2_p) || !all4(diag_x, diag_y, diag_z, diag_p) ||
+      !all4(rhs_x, rhs_y, rhs_z, rhs_p))
+    return fail(ctx, APHID_ERR_BADARG, "null array");
+  int rc = ensure_work(ctx);
+  if (rc) return rc;
+  ctx->loaded = false;
+  if ((rc = upload4(ctx, wv(ctx, W_K2), k2_x, k2_y, k2_z, k2_p))) return rc;
+  if ((rc = upload4(ctx, wv(ctx, W_INV), diag_x, diag_y, diag_z, diag_p))) return rc;
+  if ((rc = upload4(ctx, wv(ctx, W_B), rhs_x, rhs_y, rhs_z, rhs_p))) return rc;
+  ctx->loaded = true;
+  ctx->inv_ready = false;
+  return APHID_OK;
+}
+
+// The solve on the resident k2 / diag / b (src/aphid_qmr.f90:161-409).
+int qmr_run(aphid_ctx *ctx, double qmr_target, int qmr_max_it, bool use_x, double *hist,
+            int hist_cap, aphid_info *info) {
+  if (!ctx->loaded) return fail(ctx, APHID_ERR_STATE, "no problem loaded (aphid_gpu_qmr_load)");
+  // src/aphid.f90:208-216 rejects a negative target or iteration count
+  if (!(qmr_target >= 0.0) || qmr_max_it < 0)
+    return fail(ctx, APHID_ERR_BADARG, "qmr_target and qmr_max_it must be non-negative");
+  if (hist && hist_cap < 0) return fail(ctx, APHID_ERR_BADARG, "negative hist_cap");
+  const int want = std::max(1, qmr_max_it);
+  if (ctx->hist_alloc < want) {
+    cudaFree(ctx->d_hist);
+    ctx->d_hist = nullptr;
+    ctx->hist_alloc = 0;
+    CK(cudaMalloc(&ctx->d_hist, (size_t)want * sizeof(double)));
+    ctx->hist_alloc = want;
+  }
+  const long long n = ctx->n;
+  const int sb = ctx->sblk;
+  double2 *k2 = wv(ctx, W_K2), *inv = wv(ctx, W_INV), *b = wv(ctx, W_B), *x = wv(ctx, W_X);
+  double2 *r = wv(ctx, W_R), *s = wv(ctx, W_S), *p = wv(ctx, W_P), *d = wv(ctx, W_D);
+  double2 *v = wv(ctx, W_V), *q = wv(ctx, W_Q);
+  long long nlaunch = 3;  // rhsnorm, init_r, init_v
+
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (!use_x) CK(cudaMemsetAsync(x, 0, n * sizeof(double2), ctx->stream));
+  Scal64 h{};
+  h.c_n = 1.0;
+  h.eps = make_double2(1.0, 0.0);
+  h.theta_n = 0.0;
+  h.eta = make_double2(-1.0, 0.0);
+  h.iter = 1;
+  h.max_it = qmr_max_it;
+  h.target = qmr_target;
+  h.hist_cap = ctx->hist_alloc;
+  CK(cudaMemcpyAsync(ctx->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(p, 0, n * sizeof(double2), ctx->stream));
+  CK(cudaMemsetAsync(d, 0, n * sizeof(double2), ctx->stream));
+  CK(cudaMemsetAsync(s, 0, n * sizeof(double2), ctx->stream));
+  k_rhsnorm64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, b, ctx->d_sc, ctx->d_part, ctx->d_cnt + 4);
+  if (!ctx->inv_ready) {
+    k_invert64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, inv, inv);
+    ctx->inv_ready = true;
+    nlaunch++;
+  }
+  if (use_x) {
+    launch_apply(ctx, k2, x, q);
+    nlaunch++;
+  }
+  k_init_r64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, b, use_x ? q : nullptr, r, ctx->d_sc,
+                                                     ctx->d_part, ctx->d_cnt + 5);
+  k_init_v64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, r, inv, v, ctx->d_sc, ctx->d_part,
+                                                     ctx->d_cnt + 6);
+  CK(cudaGetLastError());
+  int rc = build_graph(ctx);
+  if (rc) return rc;
+
+  // replay the captured iterations until the device-side stop test fires
+  const long long max_launch = (long long)std::max(1, qmr_max_it) / ctx->graph_iters + 3;
+  long long launches = 0;
+  for (;;) {
+    CK(cudaMemcpyAsync(ctx->h_done, &ctx->d_sc->done, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->h_done) break;
+    if (launches++ > max_launch) return fail(ctx, APHID_ERR_STATE, "iteration loop did not terminate");
+    CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+    nlaunch += 4LL * ctx->graph_iters;
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  nlaunch += 2;
+  // true FP64 residual of the returned x
+  launch_apply(ctx, k2, x, q);
+  k_resid64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, b, q, ctx->d_out, ctx->d_part, ctx->d_cnt + 7);
+  CK(cudaGetLastError());
+  double rr = 0.0;
+  CK(cudaMemcpyAsync(&h, ctx->d_sc, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&rr, ctx->d_out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  const int nh = std::min(h.nhist, hist ? hist_cap : 0);
+  if (nh > 0) CK(cudaMemcpyAsync(hist, ctx->d_hist, nh * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  if (info) {
+    info->status = h.status;
+    info->iters = h.iter;
+    info->inner_iters = h.nhist;
+    info->outer_iters = 1;
+    info->rhs_norm = h.rhsnorm;
+    info->recur_resid = h.rnorm;
+    info->true_rel_resid = h.rhsnorm > 0 ? std::sqrt(rr) / h.rhsnorm : std::sqrt(rr);
+    info->seconds = ms * 1e-3;
+    info->kernel_launches = nlaunch;
+  }
+  return APHID_OK;
+}
+
+}  // namespace
+
+int aphid_gpu_qmr_load(aphid_ctx *ctx, const aphid_z *k2_x, const aphid_z *k2_y, const aphid_z *k2_z,
+                       const aphid_z *k2_p, const aphid_z *diag_x, const aphid_z *diag_y,
+                       const aphid_z *diag_z, const aphid_z *diag_p, const aphid_z *rhs_x,
+                       const aphid_z *rhs_y, const aphid_z *rhs_z, const aphid_z *rhs_p) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if ((rc = qmr_load(ctx, k2_x, k2_y, k2_z, k2_p, diag_x, diag_y, diag_z, diag_p, rhs_x, rhs_y, rhs_z,
+                     rhs_p)))
+    return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+int aphid_gpu_qmr_run(aphid_ctx *ctx, double qmr_target, int qmr_max_it, int use_previous_x,
+                      double *hist, int hist_cap, aphid_info *info) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  return qmr_run(ctx, qmr_target, qmr_max_it, use_previous_x != 0, hist, hist_cap, info);
+}
+
+int aphid_gpu_qmr_fetch(aphid_ctx *ctx, aphid_z *sol_x, aphid_z *sol_y, aphid_z *sol_z,
+                        aphid_z *sol_p) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->loaded) return fail(ctx, APHID_ERR_STATE, "no problem loaded");
+  if (!all4(sol_x, sol_y, sol_z, sol_p)) return fail(ctx, APHID_ERR_BADARG, "null array");
+  if ((rc = download4(ctx, wv(ctx, W_X), sol_x, sol_y, sol_z, sol_p))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+int aphid_gpu_qmr(aphid_ctx *ctx, const aphid_z *k2_x, const aphid_z *k2_y, const aphid_z *k2_z,
+                  const aphid_z *k2_p, const aphid_z *diag_x, const aphid_z *diag_y,
+                  const aphid_z *diag_z, const aphid_z *diag_p, aphid_z *rhs_x, aphid_z *rhs_y,
+                  aphid_z *rhs_z, aphid_z *rhs_p, const aphid_z *x0_x, const aphid_z *x0_y,
+                  const aphid_z *x0_z, const aphid_z *x0_p, double qmr_target, int qmr_max_it,
+                  double *hist, int hist_cap, aphid_info *info) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  const bool any_x0 = x0_x || x0_y || x0_z || x0_p;
+  if (any_x0 && !all4(x0_x, x0_y, x0_z, x0_p))
+    return fail(ctx, APHID_ERR_BADARG, "x0 must be all four blocks or none");
+  if (!(qmr_target >= 0.0) || qmr_max_it < 0)
+    return fail(ctx, APHID_ERR_BADARG, "qmr_target and qmr_max_it must be non-negative");
+  if ((rc = qmr_load(ctx, k2_x, k2_y, k2_z, k2_p, diag_x, diag_y, diag_z, diag_p, rhs_x, rhs_y, rhs_z,
+                     rhs_p)))
+    return rc;
+  if (any_x0 && (rc = upload4(ctx, wv(ctx, W_X), x0_x, x0_y, x0_z, x0_p))) return rc;
+  if ((rc = qmr_run(ctx, qmr_target, qmr_max_it, any_x0, hist, hist_cap, info))) return rc;
+  if ((rc = download4(ctx, wv(ctx, W_X), rhs_x, rhs_y, rhs_z, rhs_p))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+int aphid_gpu_inprod_dev(aphid_ctx *ctx, const void *d_k2, const void *d_in, void *d_out,
+                         void *d_eps) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!d_k2 || !d_in || !d_out) return fail(ctx, APHID_ERR_BADARG, "null device pointer");
+  if ((rc = ensure_work(ctx))) return rc;
+  const unsigned nb = (unsigned)ctx->tiles.count();
+  if (d_eps)
+    k_apply64<kApplyEps><<<nb, kOpThreads, 0, ctx->stream>>>(
+        ctx->g, ctx->tiles, (const double2 *)d_k2, (const double2 *)d_in, (double2 *)d_out, nullptr,
+        (double2 *)d_eps, ctx->d_part, ctx->d_cnt + 8);
+  else
+    launch_apply(ctx, (const double2 *)d_k2, (const double2 *)d_in, (double2 *)d_out);
+  CK(cudaGetLastError());
+  return APHID_OK;
+}
+
+int aphid_gpu_fields(aphid_ctx *ctx, double omega, const aphid_z *a_x, const aphid_z *a_y,
+                     const aphid_z *a_z, const aphid_z *phi, aphid_z *b_x, aphid_z *b_y, aphid_z *b_z,
+                     aphid_z *e_x, aphid_z *e_y, aphid_z *e_z) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!all4(a_x, a_y, a_z, phi)) return fail(ctx, APHID_ERR_BADARG, "null potential array");
+  if ((rc = ensure_work(ctx))) return rc;
+  ctx->loaded = false;  // the work space is reused below
+  const long long nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+  const long long nbx = nx * (ny - 1) * (nz - 1), nby = (nx - 1) * ny * (nz - 1);
+  const long long nbz = (nx - 1) * (ny - 1) * nz;
+  double2 *a = wv(ctx, W_P), *bx = wv(ctx, W_Q), *by = bx + nbx, *bz = by + nby;
+  double2 *e = wv(ctx, W_R);
+  if ((rc = upload4(ctx, a, a_x, a_y, a_z, phi))) return rc;
+  k_fields<<<node_grid(ctx), 128, 0, ctx->stream>>>(ctx->g, omega, a, b_x ? bx : nullptr,
+                                                     b_y ? by : nullptr, b_z ? bz : nullptr,
+                                                     e_x ? e + ctx->g.ox : nullptr,
+                                                     e_y ? e + ctx->g.oy : nullptr,
+                                                     e_z ? e + ctx->g.oz : nullptr);
+  CK(cudaGetLastError());
+  auto dl = [&](aphid_z *dst, const double2 *src, long long cnt) -> int {
+    if (dst) CK(cudaMemcpyAsync(dst, src, cnt * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+    return APHID_OK;
+  };
+  if ((rc = dl(b_x, bx, nbx)) || (rc = dl(b_y, by, nby)) || (rc = dl(b_z, bz, nbz))) return rc;
+  if ((rc = dl(e_x, e + ctx->g.ox, ctx->g.oy - ctx->g.ox)) || (rc = dl(e_y, e + ctx->g.oy, ctx->g.oz - ctx->g.oy)) ||
+      (rc = dl(e_z, e + ctx->g.oz, ctx->g.op - ctx->g.oz)))
+    return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+}  // extern "C"

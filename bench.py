@@ -1,0 +1,307 @@
+"""Benchmark: time-to-residual-1e-8 of APhiD's frequency-domain solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload hetero96] [--precision fp64]
+
+One step = one full solve of the workload to relative residual 1e-8 from a
+zero start.  `value` = sweeps per second over all ranks, measured on device
+with CUDA events, inputs resident in HBM (aphid_gpu_qmr_run); `e2e` = the same
+through the public host-buffer call (aphid_gpu_qmr: host->device copies of
+k^2, the Jacobi diagonal and b, device->host copy of the solution, inside the
+timed region).  The working set (10 complex128 vectors of 3.6 M unknowns,
+580 MB) is larger than L2, so no explicit flush is needed.
+
+Multi-GPU: one process per GPU, each solving its own sweep (the reference's
+MPI farm is an embarrassingly parallel split over frequencies x sources), no
+collective in the solve; value = sweeps of all ranks / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-residual-1e-8 per frequency sweep (reported as sweeps/s) and QMR iters/s"
+TARGET = 1e-8
+MAX_IT = 20000
+# Iterations to relative residual 1e-8 of the complex128 Jacobi-QMR (the
+# reference's own recurrence and stop test) on each workload, measured on the
+# B200 complex128 path, which reproduces the reference's iteration count.  The
+# CPU arms time a bounded number of iterations and extrapolate with it.
+FP64_ITERS = {"halfspace32": None, "hetero96": None}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                t = [x.strip() for x in line.split(",")]
+                if len(t) >= 9:
+                    rows.append(t)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def setup_problem(workload):
+    from aphid_git_b200 import model
+    m = model.make_model(workload)
+    w = 2 * np.pi * float(m.freqs[0])
+    sig = model.sigma_hat("R", w, m.sig_re.ravel(order="F"))
+    b, _ = model.gen_rhs(m.xn, m.yn, m.zn, 5, m.sources[0])
+    return m, w, sig, b
+
+
+def cpu_port_sample(workload, iters, threads=4):
+    """The oracle's 4-thread component split (the reference's qmr_mthread
+    parallelism, src/aphid_qmr.f90:744-928) for `iters` iterations.
+    Returns seconds per iteration."""
+    from oracle import oracle as O
+    m, w, sig, b = setup_problem(workload)
+    g = O.Grid(m.xn, m.yn, m.zn)
+    k2 = O.gen_k2(g, sig, w)
+    diag = O.gen_diag(g, k2)
+    r = O.qmr(g, k2, diag, b, 1e-30, iters, nthreads=threads)
+    return r["seconds"] / max(1, len(r["hist"])), len(r["hist"])
+
+
+def run_reference(args):
+    """--impl reference: the CPU port of the reference's path (no Fortran
+    compiler exists here, so oracle/_ref cannot be built)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    iters = FP64_ITERS.get(args.workload)
+    sample_it = args.cpu_sample_iters
+    times = []
+    for step in range(args.warmup + args.steps):
+        spi, done = cpu_port_sample(args.workload, sample_it)
+        if step >= args.warmup:
+            times.append(spi)
+    spi = float(np.mean(times))
+    value = 1.0 / (spi * iters) if iters else None
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": spi * iters * 1e3 if iters else None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": args.workload, "target": TARGET},
+        "s_per_iter": spi, "iters_to_tol": iters,
+        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": 4, "kind": "port",
+                         "sample": "%d QMR iterations per step, 4-thread component split; "
+                                   "time-to-tolerance = s/iter x %s iterations" % (sample_it, iters)},
+        "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hetero96")
+    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--cpu-sample-iters", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    from aphid_git_b200 import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    # a real stream (not the NULL stream) shared by the library and the
+    # CUDA events, so the events bracket the library's kernels
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    m, w, sig, b = setup_problem(args.workload)
+    s = Solver(device=local, stream=stream.cuda_stream)
+    s.set_nodes(m.xn, m.yn, m.zn)
+    k2 = s.gen_k2(sig, w)
+    diag = s.gen_diag(k2)
+    n = s.n
+
+    # ---- resident solve: value
+    s.qmr_load(k2, diag, b)
+    for _ in range(args.warmup):
+        info, _ = s.qmr_run(TARGET, MAX_IT)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    infos = []
+    for _ in range(args.steps):
+        info, _ = s.qmr_run(TARGET, MAX_IT)
+        infos.append(info)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    iters = infos[-1]["iters"]
+    sweeps = world * args.steps
+    value = sweeps / (ms * 1e-3)
+    launches = int(sum(i["kernel_launches"] for i in infos))
+
+    # ---- public host-buffer call: e2e
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(args.steps):
+        x, info_e, _ = s.qmr(k2, diag, b, TARGET, MAX_IT, hist=False)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms_e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e = float(t.item())
+    e2e = {"value": sweeps / (ms_e * 1e-3), "unit": "sweeps/s",
+           "h2d_bytes_per_step": 3 * 16 * n, "d2h_bytes_per_step": 16 * n}
+
+    # ---- roofline of the dominant kernel: the operator apply of a QMR step
+    # (q = K p with epsilon = p^T q reduced in the same pass), timed alone on
+    # the library's stream with CUDA events.  Algorithmic bytes per launch:
+    # read p and k^2, write q: 3 x 16 B per unknown.
+    kt = torch.from_numpy(k2.view(np.float64)).to(dev)
+    pt = torch.randn(2 * n, dtype=torch.float64, device=dev)
+    qt = torch.empty(2 * n, dtype=torch.float64, device=dev)
+    et = torch.empty(2, dtype=torch.float64, device=dev)
+    reps = 50
+    for _ in range(5):
+        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(reps):
+        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    t_apply = e0.elapsed_time(e1) * 1e-3 / reps
+    peak, peak_kind = peaks()
+    alg = 3 * 16 * n
+    achieved = alg / t_apply / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("apply64_qmr_" + args.workload)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded generator, no public dataset)",
+        "config": {"workload": args.workload, "precision": args.precision, "unknowns": n,
+                   "target": TARGET, "l2": "working set > L2 (126 MB), no flush",
+                   "parallelism": "independent sweep per GPU"},
+        "time_to_tol_s": ms / args.steps * 1e-3, "iters_to_tol": iters,
+        "qmr_iters_per_s": world * args.steps * iters / (ms * 1e-3),
+        "true_rel_resid": infos[-1]["true_rel_resid"], "status": infos[-1]["status_name"],
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        "roofline": {"bound": "hbm", "kernel": "k_apply64 (QMR step)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
+                     "traffic": traffic, "alg_bytes_per_launch": alg,
+                     "launch_us": t_apply * 1e6},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        spi, done = cpu_port_sample(args.workload, args.cpu_sample_iters)
+        line["cpu_baseline"] = {
+            "value": 1.0 / (spi * iters), "unit": "sweeps/s", "cores": 4, "kind": "port",
+            "sample": "%d QMR iterations of the workload, oracle 4-thread component split; "
+                      "time-to-tolerance = %.3f s/iter x %d iterations (GPU count, same recurrence)"
+                      % (done, spi, iters),
+            "s_per_iter": spi}
+    s.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

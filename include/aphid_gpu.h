@@ -1,0 +1,193 @@
+/*
+ * aphid_gpu.h -- C ABI of the B200 (sm_100a) implementation of APhiD's
+ * frequency-domain solve: the matrix-free Lorenz-gauged A-Phi operator on the
+ * staggered Yee grid and the Jacobi-preconditioned complex-symmetric QMR
+ * that inverts it.
+ *
+ * The ABI uses plain C types only, so a Fortran host can bind it with
+ * ISO_C_BINDING (fortran/aphid_gpu_mod.f90) and Python with ctypes.
+ *
+ * Conventions
+ *   - aphid_z is layout-identical to Fortran complex(c_double_complex) and to
+ *     C99 double _Complex.
+ *   - Every array is Fortran column-major with the reference's shapes:
+ *       Ax, k2_x, diag_x, rhs_x : (nx-1, ny,   nz  )   x-directed edges
+ *       Ay, ...                 : (nx,   ny-1, nz  )   y-directed edges
+ *       Az, ...                 : (nx,   ny,   nz-1)   z-directed edges
+ *       Phi, ...                : (nx,   ny,   nz  )   nodes
+ *       cells (sigma)           : (nx-1, ny-1, nz-1)
+ *     (nx, ny, nz are NODE counts, as in the reference's aphid.mesh.)
+ *   - dx, dy, dz are dx(0:nx) etc. (nx+1 values); dxc, dyc, dzc are
+ *     dxc(1:nx) etc. (nx values), exactly the module mesh arrays
+ *     (src/aphid_mod.f90:44-45, filled by src/aphid.f90:341-361).
+ *   - Host pointers belong to the caller; the library copies in and out and
+ *     keeps no host pointer after a call returns.
+ *   - Calls are synchronous and never abort the process.  They return
+ *     APHID_OK (0) or a negative APHID_ERR_* code; aphid_gpu_last_error()
+ *     gives the message.  Solver outcomes (converged, iteration cap,
+ *     breakdown) are reported in aphid_info.status, not as errors, because
+ *     the reference only warns on non-convergence
+ *     (src/aphid_qmr.f90:394-401).
+ *   - One context per host thread.
+ */
+#ifndef APHID_GPU_H
+#define APHID_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { double re, im; } aphid_z;
+typedef struct aphid_ctx aphid_ctx;
+
+/* call results */
+#define APHID_OK             0
+#define APHID_ERR_BADARG    -1   /* invalid argument (sizes, pointers, flags) */
+#define APHID_ERR_CUDA      -2   /* CUDA runtime error, message in last_error */
+#define APHID_ERR_NOMEM     -3   /* device allocation failed */
+#define APHID_ERR_STATE     -4   /* call order: e.g. solve before set_mesh */
+#define APHID_ERR_NODEVICE  -5   /* no usable sm_100 device */
+
+/* aphid_info.status */
+#define APHID_CONVERGED      0   /* residual below target */
+#define APHID_MAXIT          1   /* iteration cap reached (reference warns) */
+#define APHID_BREAKDOWN      2   /* QMR breakdown: delta, epsilon, beta or rho = 0 */
+#define APHID_NONFINITE      3   /* NaN/Inf in a recurrence scalar */
+
+/* precision of aphid_gpu_sweep */
+#define APHID_PREC_FP64      0   /* plain complex128 Jacobi-QMR, the reference's algorithm */
+#define APHID_PREC_MIXED     1   /* complex64 inner QMR inside FP64 defect correction */
+
+typedef struct {
+  int device;        /* CUDA device ordinal */
+  void *stream;      /* cudaStream_t to run on; NULL = a stream owned by the context */
+  int graph_iters;   /* QMR iterations per CUDA-graph launch; 0 = default (16) */
+  int verbose;       /* 1 = progress lines on stderr */
+} aphid_opts;
+
+typedef struct {
+  int status;               /* APHID_CONVERGED / MAXIT / BREAKDOWN / NONFINITE */
+  int iters;                /* iteration count as the reference reports it */
+  int inner_iters;          /* total inner (complex64) iterations, mixed path */
+  int outer_iters;          /* defect-correction steps, mixed path */
+  double rhs_norm;          /* ||b||_2 */
+  double recur_resid;       /* last recurrence residual norm ||r|| (absolute) */
+  double true_rel_resid;    /* ||b - K x||_2 / ||b||_2 recomputed in FP64 */
+  double seconds;           /* device time of the solve (CUDA events) */
+  long long kernel_launches; /* kernels this call launched (graph nodes included) */
+} aphid_info;
+
+/* ---- context --------------------------------------------------------- */
+
+/* Create a context on opts->device (opts may be NULL: device 0, own stream). */
+int aphid_gpu_create(aphid_ctx **ctx, const aphid_opts *opts);
+int aphid_gpu_destroy(aphid_ctx *ctx);
+/* Message of the last failed call on this context (never NULL). */
+const char *aphid_gpu_last_error(const aphid_ctx *ctx);
+
+/* Mesh geometry: the module mesh arrays (src/aphid_mod.f90:40-45).
+ * Requires nx, ny, nz >= 3 and positive spacings. */
+int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz,
+                       const double *dx, const double *dy, const double *dz,
+                       const double *dxc, const double *dyc, const double *dzc);
+
+/* ---- operator-level entry points -------------------------------------- */
+
+/* out = K in for all four blocks: replaces inprod_x/inprod_y/inprod_z/
+ * inprod_p (src/aphid.f90:803-871, 932-1000, 1061-1128, 1191-1282) with the
+ * coefficient tables of gen_inprod_*_coefs (src/aphid.f90:750-1185). */
+int aphid_gpu_inprod(aphid_ctx *ctx,
+                     const aphid_z *k2_x, const aphid_z *k2_y,
+                     const aphid_z *k2_z, const aphid_z *k2_p,
+                     const aphid_z *in_x, const aphid_z *in_y,
+                     const aphid_z *in_z, const aphid_z *in_p,
+                     aphid_z *out_x, aphid_z *out_y, aphid_z *out_z,
+                     aphid_z *out_p);
+
+/* k^2 grids from cell sigma-hat: replaces gen_k2_xgrid/_ygrid/_zgrid/_pgrid
+ * (src/aphid.f90:1289-1535).  sig: complex cell array (nx-1,ny-1,nz-1). */
+int aphid_gpu_gen_k2(aphid_ctx *ctx, const aphid_z *sig, double omega,
+                     aphid_z *k2_x, aphid_z *k2_y, aphid_z *k2_z,
+                     aphid_z *k2_p);
+
+/* Jacobi diagonal: replaces gen_diag (src/aphid.f90:1542-1725). */
+int aphid_gpu_gen_diag(aphid_ctx *ctx,
+                       const aphid_z *k2_x, const aphid_z *k2_y,
+                       const aphid_z *k2_z, const aphid_z *k2_p,
+                       aphid_z *diag_x, aphid_z *diag_y, aphid_z *diag_z,
+                       aphid_z *diag_p);
+
+/* ---- the solve ---------------------------------------------------------- */
+
+/* Drop-in for `call qmr` / `call qmr_mthread` (src/aphid.f90:102-104;
+ * solver src/aphid_qmr.f90:5-434).  rhs_* hold b on entry and the solution on
+ * return, exactly as the reference overwrites rhs_* (src/aphid_qmr.f90:225-240).
+ * Same recurrence, same stopping rule (recurrence residual
+ * < qmr_target * ||b||, src/aphid_qmr.f90:386-390) and the same iteration
+ * count semantics, in complex128 on the GPU.
+ * x0_* (all NULL, or all non-NULL) is an optional initial guess; the
+ * reference starts from zero (src/aphid_qmr.f90:230-233).
+ * hist (nullable) receives the recurrence residual of each iteration (the
+ * content of qmr.iter, src/aphid_qmr.f90:381), up to hist_cap values;
+ * info->iters tells how many were written (min(iters, hist_cap) when
+ * converged).  info may be NULL. */
+int aphid_gpu_qmr(aphid_ctx *ctx,
+                  const aphid_z *k2_x, const aphid_z *k2_y,
+                  const aphid_z *k2_z, const aphid_z *k2_p,
+                  const aphid_z *diag_x, const aphid_z *diag_y,
+                  const aphid_z *diag_z, const aphid_z *diag_p,
+                  aphid_z *rhs_x, aphid_z *rhs_y, aphid_z *rhs_z,
+                  aphid_z *rhs_p,
+                  const aphid_z *x0_x, const aphid_z *x0_y,
+                  const aphid_z *x0_z, const aphid_z *x0_p,
+                  double qmr_target, int qmr_max_it,
+                  double *hist, int hist_cap, aphid_info *info);
+
+/* The same solve split in three, for callers that keep a problem resident
+ * on the device and re-solve it (benchmarks, restarts):
+ *   aphid_gpu_qmr_load   copies k2_*, diag_* and rhs_* (= b) to the device,
+ *   aphid_gpu_qmr_run    runs the solve on the resident copies (x0 = 0, or
+ *                        the resident solution when use_previous_x != 0),
+ *   aphid_gpu_qmr_fetch  copies the solution back into sol_*.
+ * aphid_gpu_qmr is exactly load + run + fetch. */
+int aphid_gpu_qmr_load(aphid_ctx *ctx,
+                       const aphid_z *k2_x, const aphid_z *k2_y,
+                       const aphid_z *k2_z, const aphid_z *k2_p,
+                       const aphid_z *diag_x, const aphid_z *diag_y,
+                       const aphid_z *diag_z, const aphid_z *diag_p,
+                       const aphid_z *rhs_x, const aphid_z *rhs_y,
+                       const aphid_z *rhs_z, const aphid_z *rhs_p);
+int aphid_gpu_qmr_run(aphid_ctx *ctx, double qmr_target, int qmr_max_it,
+                      int use_previous_x, double *hist, int hist_cap,
+                      aphid_info *info);
+int aphid_gpu_qmr_fetch(aphid_ctx *ctx, aphid_z *sol_x, aphid_z *sol_y,
+                        aphid_z *sol_z, aphid_z *sol_p);
+
+/* Device-pointer form of aphid_gpu_inprod for callers whose vectors already
+ * live on this context's device (e.g. framework tensors): d_k2, d_in, d_out
+ * are concatenated [x|y|z|p] complex128 vectors of the mesh's unknown count.
+ * When d_eps is non-NULL the bilinear form in^T out (unconjugated, the
+ * epsilon of src/aphid_qmr.f90:329) is reduced on the device and written
+ * there as one aphid_z.  The reduction uses the context's scratch buffers.
+ * Runs on the context's stream; returns after the launch (asynchronous). */
+int aphid_gpu_inprod_dev(aphid_ctx *ctx, const void *d_k2, const void *d_in,
+                         void *d_out, void *d_eps);
+
+/* ---- post-processing ---------------------------------------------------- */
+
+/* B = curl A on cell faces and E = -i omega (A - grad Phi) on edges:
+ * replaces gen_fields (src/aphid.f90:2173-2252).  Shapes:
+ * Bx (nx,ny-1,nz-1), By (nx-1,ny,nz-1), Bz (nx-1,ny-1,nz); Ex/Ey/Ez the edge
+ * shapes.  Any output pointer may be NULL to skip it. */
+int aphid_gpu_fields(aphid_ctx *ctx, double omega,
+                     const aphid_z *a_x, const aphid_z *a_y,
+                     const aphid_z *a_z, const aphid_z *phi,
+                     aphid_z *b_x, aphid_z *b_y, aphid_z *b_z,
+                     aphid_z *e_x, aphid_z *e_y, aphid_z *e_z);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* APHID_GPU_H */
