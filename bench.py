@@ -36,7 +36,7 @@ MAX_IT = 20000
 # reference's own recurrence and stop test) on each workload, measured on the
 # B200 complex128 path, which reproduces the reference's iteration count.  The
 # CPU arms time a bounded number of iterations and extrapolate with it.
-FP64_ITERS = {"halfspace32": None, "hetero96": None}
+FP64_ITERS = {"halfspace32": 360, "hetero96": 1088}
 
 
 def peaks():
