@@ -149,6 +149,33 @@ def run_reference(args):
     return 0
 
 
+def time_apply(s, k2, n, dev, stream, reps=50):
+    """Seconds per launch of the QMR-step operator apply (q = K p and
+    epsilon = p^T q in one pass) on the library's stream, CUDA events."""
+    import torch
+    kt = torch.from_numpy(k2.view(np.float64)).to(dev)
+    pt = torch.randn(2 * n, dtype=torch.float64, device=dev)
+    qt = torch.empty(2 * n, dtype=torch.float64, device=dev)
+    et = torch.empty(2, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    for _ in range(5):
+        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) * 1e-3 / reps
+
+
+def only_apply(s, k2, n, dev, stream):
+    t = time_apply(s, k2, n, dev, stream, reps=10)
+    print(json.dumps({"apply_us": t * 1e6, "unknowns": n, "alg_GBps": 48 * n / t / 1e9}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -159,6 +186,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64"])
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-apply", action="store_true",
+                    help="set up the workload and time only the operator apply (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -195,6 +224,9 @@ def main():
     k2 = s.gen_k2(sig, w)
     diag = s.gen_diag(k2)
     n = s.n
+
+    if args.only_apply:
+        return only_apply(s, k2, n, dev, stream)
 
     # ---- resident solve: value
     s.qmr_load(k2, diag, b)
@@ -246,20 +278,7 @@ def main():
     # (q = K p with epsilon = p^T q reduced in the same pass), timed alone on
     # the library's stream with CUDA events.  Algorithmic bytes per launch:
     # read p and k^2, write q: 3 x 16 B per unknown.
-    kt = torch.from_numpy(k2.view(np.float64)).to(dev)
-    pt = torch.randn(2 * n, dtype=torch.float64, device=dev)
-    qt = torch.empty(2 * n, dtype=torch.float64, device=dev)
-    et = torch.empty(2, dtype=torch.float64, device=dev)
-    reps = 50
-    for _ in range(5):
-        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
-    torch.cuda.synchronize(dev)
-    e0.record(stream)
-    for _ in range(reps):
-        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    t_apply = e0.elapsed_time(e1) * 1e-3 / reps
+    t_apply = time_apply(s, k2, n, dev, stream)
     peak, peak_kind = peaks()
     alg = 3 * 16 * n
     achieved = alg / t_apply / 1e9
