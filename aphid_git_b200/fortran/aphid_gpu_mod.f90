@@ -1,0 +1,144 @@
+!======================================================================!
+! aphid_gpu_mod.f90 -- ISO_C_BINDING interface to libaphid_gpu.so      !
+! (include/aphid_gpu.h) and qmr_gpu, a drop-in for `call qmr` /          !
+! `call qmr_mthread` in aphid_main (src/aphid.f90:102-104).             !
+!                                                                      !
+! qmr_gpu takes the same module data as qmr (module mesh: nx,ny,nz,     !
+! dx,dy,dz,dxc,dyc,dzc, k2_*grid, diag_*, rhs_*; module general:        !
+! qmr_target, qmr_max_it, pwd, iout), overwrites rhs_* with the         !
+! solution, and writes qmr.iter and the stdout summary from the        !
+! returned residual history (src/aphid_qmr.f90:161-409).               !
+!                                                                      !
+! Build (where a Fortran compiler exists):                              !
+!   gfortran -c aphid_gpu_mod.f90 (after aphid_mod.f90), link with      !
+!   -L<dir> -laphid_gpu -Wl,-rpath,<dir>                                 !
+!======================================================================!
+
+      module aphid_gpu
+      use iso_c_binding
+      implicit none
+
+      integer(c_int), parameter :: APHID_OK = 0
+      integer(c_int), parameter :: APHID_CONVERGED = 0
+      integer(c_int), parameter :: APHID_MAXIT = 1
+
+      type, bind(C) :: aphid_opts
+        integer(c_int) :: device
+        type(c_ptr)    :: stream
+        integer(c_int) :: graph_iters
+        integer(c_int) :: verbose
+      end type aphid_opts
+
+      type, bind(C) :: aphid_info
+        integer(c_int)       :: status, iters, inner_iters, outer_iters
+        real(c_double)       :: rhs_norm, recur_resid, true_rel_resid
+        real(c_double)       :: seconds
+        integer(c_long_long) :: kernel_launches
+      end type aphid_info
+
+      interface
+        integer(c_int) function aphid_gpu_create(ctx, opts)             &
+                       bind(C, name="aphid_gpu_create")
+          import :: c_int, c_ptr, aphid_opts
+          type(c_ptr), intent(out) :: ctx
+          type(aphid_opts), intent(in) :: opts
+        end function
+
+        integer(c_int) function aphid_gpu_destroy(ctx)                  &
+                       bind(C, name="aphid_gpu_destroy")
+          import :: c_int, c_ptr
+          type(c_ptr), value :: ctx
+        end function
+
+        integer(c_int) function aphid_gpu_set_mesh(ctx, nx, ny, nz,     &
+                       dx, dy, dz, dxc, dyc, dzc)                       &
+                       bind(C, name="aphid_gpu_set_mesh")
+          import :: c_int, c_ptr, c_double
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: nx, ny, nz
+          real(c_double), intent(in) :: dx(*), dy(*), dz(*)
+          real(c_double), intent(in) :: dxc(*), dyc(*), dzc(*)
+        end function
+
+        integer(c_int) function aphid_gpu_qmr(ctx,                      &
+                       k2x, k2y, k2z, k2p, dgx, dgy, dgz, dgp,          &
+                       rx, ry, rz, rp, x0x, x0y, x0z, x0p,              &
+                       target, max_it, hist, hist_cap, info)            &
+                       bind(C, name="aphid_gpu_qmr")
+          import :: c_int, c_ptr, c_double, c_double_complex, aphid_info
+          type(c_ptr), value :: ctx
+          complex(c_double_complex), intent(in) :: k2x(*), k2y(*)
+          complex(c_double_complex), intent(in) :: k2z(*), k2p(*)
+          complex(c_double_complex), intent(in) :: dgx(*), dgy(*)
+          complex(c_double_complex), intent(in) :: dgz(*), dgp(*)
+          complex(c_double_complex), intent(inout) :: rx(*), ry(*)
+          complex(c_double_complex), intent(inout) :: rz(*), rp(*)
+          type(c_ptr), value :: x0x, x0y, x0z, x0p
+          real(c_double), value :: target
+          integer(c_int), value :: max_it, hist_cap
+          real(c_double), intent(out) :: hist(*)
+          type(aphid_info), intent(out) :: info
+        end function
+      end interface
+
+      contains
+
+!----------------------------------------------------------------------!
+!  Drop-in for `call qmr`: same inputs (module data), same output       !
+!  (rhs_* overwritten with the solution), same qmr.iter file.           !
+!----------------------------------------------------------------------!
+      subroutine qmr_gpu
+      use general
+      use mesh
+      type(c_ptr)       :: ctx
+      type(aphid_opts)  :: opts
+      type(aphid_info)  :: info
+      integer(c_int)    :: rc
+      integer           :: i, nh
+      real(c_double), allocatable :: hist(:)
+
+      opts%device = 0
+      opts%stream = c_null_ptr
+      opts%graph_iters = 0
+      opts%verbose = 0
+      rc = aphid_gpu_create(ctx, opts)
+      if (rc.ne.APHID_OK) then
+        write(iout,*) '>> ERROR: no usable GPU for qmr_gpu, code ', rc
+        stop
+      end if
+      rc = aphid_gpu_set_mesh(ctx, nx, ny, nz, dx, dy, dz, dxc, dyc, dzc)
+      allocate(hist(max(1, qmr_max_it)))
+      rc = aphid_gpu_qmr(ctx, k2_xgrid, k2_ygrid, k2_zgrid, k2_pgrid,   &
+                         diag_x, diag_y, diag_z, diag_p,                &
+                         rhs_x, rhs_y, rhs_z, rhs_p,                    &
+                         c_null_ptr, c_null_ptr, c_null_ptr, c_null_ptr,&
+                         qmr_target, qmr_max_it, hist,                  &
+                         int(size(hist), c_int), info)
+      if (rc.ne.APHID_OK) then
+        write(iout,*) '>> ERROR: aphid_gpu_qmr failed, code ', rc
+        stop
+      end if
+
+      open(unit=11,file=trim(pwd)//'/qmr.iter',status='unknown')
+      nh = min(info%inner_iters, size(hist))
+      do i=1,nh
+        write(11,*) i, hist(i), info%seconds
+      end do
+      close(11)
+
+      if (info%status.eq.APHID_CONVERGED) then
+        write(iout,*) 'Solution converged in ',info%iters,' iterations'
+      else
+        write(iout,*) '********** WARNING ************'
+        write(iout,*) '  Maximum iterations exceeded  '
+        write(iout,*) '*******************************'
+      end if
+      write(iout,'(a,1x,e11.4)') '   Residual:',info%recur_resid
+      write(iout,*) 'Time spent in QMR [s]: ', info%seconds
+      write(iout,*) 'Seconds per iteration:    ',                       &
+                    info%seconds/real(max(1,info%iters))
+      deallocate(hist)
+      rc = aphid_gpu_destroy(ctx)
+      end subroutine qmr_gpu
+
+      end module aphid_gpu
