@@ -76,6 +76,7 @@ def load():
     L.aphid_gpu_qmr_run.argtypes = [P, C.c_double, C.c_int, C.c_int, P, C.c_int, C.POINTER(Info)]
     L.aphid_gpu_qmr_fetch.argtypes = [P] + [_Z] * 4
     L.aphid_gpu_inprod_dev.argtypes = [P, P, P, P, P]
+    L.aphid_gpu_inprod_eps_noalloc.argtypes = [C.c_int] * 3 + [P] * 11
     _lib = L
     return L
 
@@ -97,6 +98,21 @@ def _c128(a, n=None):
     if n is not None and a.size != n:
         raise ValueError("expected %d complex values, got %d" % (n, a.size))
     return a
+
+
+NOALLOC_MAX_NODES = 1024
+
+
+def inprod_eps_noalloc(nx, ny, nz, d_spacing, d_k2, d_in, d_out, d_eps, stream=0):
+    """Allocation-free y = K x with epsilon = x^T y (aphid_gpu_inprod_eps_noalloc).
+
+    For callers that cannot allocate device memory: every argument is a device
+    pointer the caller owns (d_spacing = six pointers dx, dy, dz, dxc, dyc,
+    dzc), and the scratch is a fixed array inside the library, shared by all
+    calls (overlapping calls race).  Meshes above NOALLOC_MAX_NODES nodes per
+    axis are rejected.  Asynchronous on `stream`; returns the status code."""
+    return load().aphid_gpu_inprod_eps_noalloc(nx, ny, nz, *d_spacing, d_k2, d_in, d_out, d_eps,
+                                               stream)
 
 
 class Solver:

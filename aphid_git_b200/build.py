@@ -31,8 +31,8 @@ def up_to_date():
 def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
-    cmd = ["nvcc"] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose else []) + \
-        ["-o", LIB, os.path.join(SRC, "aphid_gpu.cu")]
+    units = [os.path.join(SRC, f) for f in ("aphid_gpu.cu", "aphid_noalloc.cu")]
+    cmd = ["nvcc"] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB] + units
     subprocess.run(cmd, check=True)
     return LIB
 

@@ -156,7 +156,7 @@ __device__ __forceinline__ double2 times_iwmu(double2 a, double omega) {
   return rmul(kMu0, rmul(omega, cmul(a, ii)));
 }
 
-__global__ void k_gen_k2(GridDev g, const double2 *__restrict__ sig, double omega,
+static __global__ void k_gen_k2(GridDev g, const double2 *__restrict__ sig, double omega,
                          double2 *__restrict__ k2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
@@ -207,7 +207,7 @@ __global__ void k_gen_k2(GridDev g, const double2 *__restrict__ sig, double omeg
 // ------------------------------------------------------- Jacobi diagonal
 // gen_diag (src/aphid.f90:1542-1725).  It uses 0.5*(d(k)+d(k-1)) where the
 // stencils use dxc, and 1 on boundary nodes.
-__global__ void k_gen_diag(GridDev g, const double2 *__restrict__ k2, double2 *__restrict__ dg) {
+static __global__ void k_gen_diag(GridDev g, const double2 *__restrict__ k2, double2 *__restrict__ dg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -265,7 +265,7 @@ __global__ void k_gen_diag(GridDev g, const double2 *__restrict__ k2, double2 *_
 // ---------------------------------------------------------------- fields
 // gen_fields (src/aphid.f90:2173-2252): B = curl A on faces,
 // E = -i omega (A - grad Phi) on edges.
-__global__ void k_fields(GridDev g, double omega, const double2 *__restrict__ a,
+static __global__ void k_fields(GridDev g, double omega, const double2 *__restrict__ a,
                          double2 *__restrict__ bx, double2 *__restrict__ by,
                          double2 *__restrict__ bz, double2 *__restrict__ ex,
                          double2 *__restrict__ ey, double2 *__restrict__ ez) {

@@ -36,7 +36,7 @@ __device__ __forceinline__ bool guard(Scal64 *sc, bool ok_finite, bool ok_nonzer
 }
 
 // ||b||^2 -> rhsnorm (src/aphid_qmr.f90:169-172)
-__global__ void __launch_bounds__(kStreamThreads) k_rhsnorm64(long long n, const double2 *__restrict__ b,
+static __global__ void __launch_bounds__(kStreamThreads) k_rhsnorm64(long long n, const double2 *__restrict__ b,
                                                             Scal64 *sc, double *part, unsigned *cnt) {
   Vals<1> a{{0.0}};
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_rhsnorm64(long long n, const
 }
 
 // inv_diag = 1/diag (src/aphid_qmr.f90:178-181)
-__global__ void k_invert64(long long n, const double2 *__restrict__ dg, double2 *__restrict__ inv) {
+static __global__ void k_invert64(long long n, const double2 *__restrict__ dg, double2 *__restrict__ inv) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x)
     inv[t] = cdiv(make_double2(1.0, 0.0), dg[t]);
@@ -58,7 +58,7 @@ __global__ void k_invert64(long long n, const double2 *__restrict__ dg, double2 
 
 // r = b - q (q = K x0, or absent for a zero start); ||r|| -> rho_np
 // (src/aphid_qmr.f90:245-263)
-__global__ void __launch_bounds__(kStreamThreads) k_init_r64(long long n, const double2 *__restrict__ b,
+static __global__ void __launch_bounds__(kStreamThreads) k_init_r64(long long n, const double2 *__restrict__ b,
                                                            const double2 *__restrict__ q,
                                                            double2 *__restrict__ r, Scal64 *sc,
                                                            double *part, unsigned *cnt) {
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_init_r64(long long n, const 
 
 // v = r/rho; delta = v^T M^-1 v for the first iteration, then the loop-top
 // assignments (src/aphid_qmr.f90:268-285, 299-313)
-__global__ void __launch_bounds__(kStreamThreads) k_init_v64(long long n, const double2 *__restrict__ r,
+static __global__ void __launch_bounds__(kStreamThreads) k_init_v64(long long n, const double2 *__restrict__ r,
                                                            const double2 *__restrict__ inv,
                                                            double2 *__restrict__ v, Scal64 *sc,
                                                            double *part, unsigned *cnt) {
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_init_v64(long long n, const 
 }
 
 // step 2: p = M^-1 v - k1 p (src/aphid_qmr.f90:306-320)
-__global__ void __launch_bounds__(kStreamThreads) k_pupd64(long long n, const double2 *__restrict__ v,
+static __global__ void __launch_bounds__(kStreamThreads) k_pupd64(long long n, const double2 *__restrict__ v,
                                                          const double2 *__restrict__ inv,
                                                          double2 *__restrict__ p, const Scal64 *sc) {
   if (sc->done) return;
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_pupd64(long long n, const do
 // written to *eps_out.
 enum { kApplyPlain = 0, kApplyQmr = 1, kApplyEps = 2 };
 template <int MODE>
-__global__ void __launch_bounds__(kOpThreads) k_apply64(GridDev g, Tiles tl,
+static __global__ void __launch_bounds__(kOpThreads) k_apply64(GridDev g, Tiles tl,
                                                       const double2 *__restrict__ k2,
                                                       const double2 *__restrict__ in,
                                                       double2 *__restrict__ out, Scal64 *sc,
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kOpThreads) k_apply64(GridDev g, Tiles tl,
 
 // step 3b + 4: rho = ||q - beta v||; theta, c, eta, kappa
 // (src/aphid_qmr.f90:332-345)
-__global__ void __launch_bounds__(kStreamThreads) k_rho64(long long n, const double2 *__restrict__ q,
+static __global__ void __launch_bounds__(kStreamThreads) k_rho64(long long n, const double2 *__restrict__ q,
                                                         const double2 *__restrict__ v, Scal64 *sc,
                                                         double *part, unsigned *cnt) {
   if (sc->done) return;
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_rho64(long long n, const dou
 
 // step 4 updates + stop test: d, x, s, r, v; ||r||; next delta and k1
 // (src/aphid_qmr.f90:347-390, 299-313)
-__global__ void __launch_bounds__(kStreamThreads) k_upd64(long long n, const double2 *__restrict__ p,
+static __global__ void __launch_bounds__(kStreamThreads) k_upd64(long long n, const double2 *__restrict__ p,
                                                         const double2 *__restrict__ q,
                                                         const double2 *__restrict__ inv,
                                                         double2 *__restrict__ d, double2 *__restrict__ x,
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(kStreamThreads) k_upd64(long long n, const dou
 }
 
 // ||b - q||^2 for the true residual of the returned solution
-__global__ void __launch_bounds__(kStreamThreads) k_resid64(long long n, const double2 *__restrict__ b,
+static __global__ void __launch_bounds__(kStreamThreads) k_resid64(long long n, const double2 *__restrict__ b,
                                                           const double2 *__restrict__ q, double *out,
                                                           double *part, unsigned *cnt) {
   Vals<1> a{{0.0}};

@@ -5,7 +5,8 @@
  * that inverts it.
  *
  * The ABI uses plain C types only, so a Fortran host can bind it with
- * ISO_C_BINDING (fortran/aphid_gpu_mod.f90) and Python with ctypes.
+ * ISO_C_BINDING (aphid_git_b200/fortran/aphid_gpu_mod.f90) and Python with
+ * ctypes (aphid_git_b200/abi.py).
  *
  * Conventions
  *   - aphid_z is layout-identical to Fortran complex(c_double_complex) and to
@@ -174,6 +175,33 @@ int aphid_gpu_qmr_fetch(aphid_ctx *ctx, aphid_z *sol_x, aphid_z *sol_y,
  * Runs on the context's stream; returns after the launch (asynchronous). */
 int aphid_gpu_inprod_dev(aphid_ctx *ctx, const void *d_k2, const void *d_in,
                          void *d_out, void *d_eps);
+
+/* ---- allocation-free operator apply -------------------------------------- */
+
+/* No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc -- code that runs inside a memory pool or a framework allocator
+ * owning all device memory, or a host that must not allocate once a run has
+ * started.  It computes the same result as aphid_gpu_inprod_dev with a
+ * non-NULL d_eps (out = K in, and the epsilon in^T out written to *d_eps as
+ * one aphid_z), but needs no context and allocates nothing: every argument
+ * is a caller-owned device pointer on the current device (d_dx..d_dzc hold
+ * dx(0:n) and dxc(1:n) as in aphid_gpu_set_mesh; d_k2, d_in, d_out are the
+ * concatenated [x|y|z|p] complex128 vectors).  Its scratch is one fixed
+ * file-scope device array of about 400 KB, held by every GPU that loads the
+ * library until the process exits; meshes larger than
+ * APHID_NOALLOC_MAX_NODES nodes per axis are rejected with APHID_ERR_BADARG.
+ * All calls share that array: calls that overlap on the GPU race on it.  The
+ * first call on a device looks the array up, so make it before any stream
+ * capture.  Runs on `stream` (a cudaStream_t, NULL = legacy default) and
+ * returns after the launch. */
+#define APHID_NOALLOC_MAX_NODES 1024
+#define APHID_NOALLOC_MAX_SLOTS 16384
+int aphid_gpu_inprod_eps_noalloc(int nx, int ny, int nz,
+                                 const double *d_dx, const double *d_dy,
+                                 const double *d_dz, const double *d_dxc,
+                                 const double *d_dyc, const double *d_dzc,
+                                 const void *d_k2, const void *d_in,
+                                 void *d_out, void *d_eps, void *stream);
 
 /* ---- post-processing ---------------------------------------------------- */
 
