@@ -26,6 +26,11 @@ class AphidError(RuntimeError):
     pass
 
 
+class SweepOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("target", C.c_double), ("max_it", C.c_int),
+                ("inner_tol", C.c_double), ("max_outer", C.c_int), ("reserved", C.c_int * 3)]
+
+
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("stream", C.c_void_p), ("graph_iters", C.c_int),
                 ("verbose", C.c_int)]
@@ -77,6 +82,11 @@ def load():
     L.aphid_gpu_qmr_fetch.argtypes = [P] + [_Z] * 4
     L.aphid_gpu_inprod_dev.argtypes = [P, P, P, P, P]
     L.aphid_gpu_inprod_eps_noalloc.argtypes = [C.c_int] * 3 + [P] * 11
+    L.aphid_gpu_set_model.argtypes = [P, C.c_char, P, P]
+    L.aphid_gpu_sweep.argtypes = [P, C.c_int, P, P, C.c_int, P, C.c_char_p, P, P,
+                                  C.POINTER(SweepOpts), P, P]
+    L.aphid_gpu_sweep_fetch.argtypes = [P, C.c_int, P]
+    L.aphid_gpu_sweep_time_apply.argtypes = [P, C.c_int]
     _lib = L
     return L
 
@@ -242,6 +252,65 @@ class Solver:
         asynchronous on the context's stream."""
         self._check(self.lib.aphid_gpu_inprod_dev(self._h, d_k2, d_in, d_out, d_eps),
                     "inprod_dev")
+
+    # ------------------------------------------------------------ sweep
+    def set_model(self, csig_flag, sig_re=None, eps_rel=None):
+        """Cell model for sweeps: 'R' (sig_re), 'C' (sig_re, eps_rel) or 'I'
+        (eps_rel); real(4) cell arrays of (nx-1)(ny-1)(nz-1) values, Fortran
+        order."""
+        nx, ny, nz = self.dims
+        nc = (nx - 1) * (ny - 1) * (nz - 1)
+
+        def f32(a):
+            if a is None:
+                return None
+            a = np.asarray(a, dtype=np.float32)
+            a = np.ascontiguousarray(a.ravel(order="F") if a.ndim == 3 else a)
+            if a.size != nc:
+                raise ValueError("cell array must have %d values" % nc)
+            return a
+        self._model = [f32(sig_re), f32(eps_rel)]
+        self._check(self.lib.aphid_gpu_set_model(
+            self._h, csig_flag.encode(),
+            self._model[0].ctypes.data if self._model[0] is not None else None,
+            self._model[1].ctypes.data if self._model[1] is not None else None), "set_model")
+
+    def sweep(self, omegas, sources, source_of_system=None, x0=None, precision="mixed",
+              target=1e-8, max_it=20000, inner_tol=0.0, max_outer=0, fetch=True):
+        """Solve all (omega, source) systems in one batched launch.
+
+        sources: list of oper_mode-5 dipole lists [(dir, i, j, k), ...];
+        source_of_system[s] picks the source of system s (default: s).
+        Returns (X, infos): X is (nsys, nunk) complex128 (None when fetch is
+        False: the solutions stay on the device, see sweep_fetch)."""
+        om = np.ascontiguousarray(np.atleast_1d(omegas), dtype=np.float64)
+        nsys = om.size
+        sos = np.ascontiguousarray(np.arange(nsys) if source_of_system is None
+                                   else source_of_system, dtype=np.int32)
+        ndip = np.array([len(q) for q in sources], dtype=np.int32)
+        dirs = "".join(str(d[0])[:2].ljust(2) for q in sources for d in q).encode()
+        ijk = np.array([[int(d[1]), int(d[2]), int(d[3])] for q in sources for d in q] or
+                       [[0, 0, 0]], dtype=np.int32)
+        x0a = None if x0 is None else np.ascontiguousarray(x0, dtype=np.complex128).reshape(nsys, self.n)
+        X = np.empty((nsys, self.n), np.complex128) if fetch else None
+        infos = (Info * nsys)()
+        o = SweepOpts(PREC_MIXED if precision == "mixed" else PREC_FP64, float(target), int(max_it),
+                      float(inner_tol), int(max_outer))
+        self._check(self.lib.aphid_gpu_sweep(
+            self._h, nsys, om.ctypes.data, sos.ctypes.data, len(sources), ndip.ctypes.data,
+            dirs or b"  ", ijk.ctypes.data, x0a.ctypes.data if x0a is not None else None,
+            C.byref(o), X.ctypes.data if X is not None else None, infos), "sweep")
+        return X, [i.as_dict() for i in infos]
+
+    def sweep_time_apply(self, reps):
+        """Launch the complex64 operator pass `reps` times on the resident
+        systems of the last mixed sweep (asynchronous; for timing)."""
+        self._check(self.lib.aphid_gpu_sweep_time_apply(self._h, int(reps)), "sweep_time_apply")
+
+    def sweep_fetch(self, sys):
+        x = np.empty(self.n, np.complex128)
+        self._check(self.lib.aphid_gpu_sweep_fetch(self._h, int(sys), x.ctypes.data), "sweep_fetch")
+        return x
 
     def gen_fields(self, omega, sol):
         """(B, E): B = curl A on faces [Bx|By|Bz], E on edges [Ex|Ey|Ez]."""

@@ -142,3 +142,25 @@ __device__ __forceinline__ Vals<NV> final_reduce(const double *partials, unsigne
 }
 
 }  // namespace aphid
+
+namespace aphid {
+// float2 counterparts of the complex helpers (complex64 inner solver)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 rmul(float r, float2 b) { return make_float2(r * b.x, r * b.y); }
+__device__ __forceinline__ float2 rdiv(float2 a, float r) { return make_float2(a.x / r, a.y / r); }
+__device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
+
+template <typename R> struct CplxOf;
+template <> struct CplxOf<float> { using T = float2; };
+template <> struct CplxOf<double> { using T = double2; };
+template <typename R>
+__device__ __forceinline__ typename CplxOf<R>::T mkc(R a, R b);
+template <> __device__ __forceinline__ float2 mkc<float>(float a, float b) { return make_float2(a, b); }
+template <> __device__ __forceinline__ double2 mkc<double>(double a, double b) { return make_double2(a, b); }
+}  // namespace aphid

@@ -10,11 +10,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
 #include "../../include/aphid_gpu.h"
-#include "aphid_qmr64.cuh"
+#include "aphid_sweep.cuh"
 
 using namespace aphid;
 
@@ -31,8 +32,10 @@ struct aphid_ctx {
   int nx = 0, ny = 0, nz = 0;
   long long n = 0;
   double *d_tab = nullptr;
+  std::vector<double> host_d[3];  // dx(0:n) per axis (host copy, for source lengths)
   GridDev g{};
   Tiles tiles{};
+  Tiles ptiles{};  // plane tiles of the complex64 operator pass
   int sblk = 0;  // blocks of the streaming kernels
 
   // complex128 work space: k2 inv b x r s p d v q
@@ -53,6 +56,27 @@ struct aphid_ctx {
   // resident problem state (aphid_gpu_qmr_load / _run / _fetch)
   bool loaded = false;     // k2, diag and b are on the device
   bool inv_ready = false;  // W_INV holds 1/diag (else diag)
+
+  // sweep model: FP64 averages per unknown, and FP32 copies for the inner loop
+  bool has_model = false;
+  char csig = 'R';
+  double *d_sig = nullptr, *d_epsr = nullptr;
+  float *d_sig32 = nullptr, *d_epsr32 = nullptr;
+  // sweep state
+  int sw_nsys = 0;           // systems the buffers hold
+  bool sw_f32_ok = false;    // complex64 vectors allocated
+  double2 *sw_f64 = nullptr; // [2][nsys][n]: x64, b
+  float2 *sw_f32 = nullptr;  // [6][nsys][n]: v p q d x s
+  SweepSys *sw_sys = nullptr;
+  double *sw_part = nullptr;
+  unsigned *sw_cnt = nullptr;
+  int *sw_ndone = nullptr;
+  int *h_ndone = nullptr;
+  long long sw_slots = 0;
+  int sw_bps = 0;
+  int sw_last = 0;           // systems in the last sweep
+  cudaGraphExec_t sw_gexec = nullptr;
+  int sw_gkey = 0;
 };
 
 namespace {
@@ -105,6 +129,23 @@ void release_work(aphid_ctx *ctx) {
   ctx->d_hist = nullptr;
   ctx->d_out = nullptr;
   ctx->hist_alloc = 0;
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  cudaFree(ctx->sw_f64);
+  cudaFree(ctx->sw_f32);
+  cudaFree(ctx->sw_sys);
+  cudaFree(ctx->sw_part);
+  cudaFree(ctx->sw_cnt);
+  cudaFree(ctx->sw_ndone);
+  ctx->sw_f64 = nullptr;
+  ctx->sw_f32 = nullptr;
+  ctx->sw_sys = nullptr;
+  ctx->sw_part = nullptr;
+  ctx->sw_cnt = nullptr;
+  ctx->sw_ndone = nullptr;
+  ctx->sw_nsys = 0;
+  ctx->sw_f32_ok = false;
+  ctx->sw_last = 0;
 }
 
 int ensure_work(aphid_ctx *ctx) {
@@ -231,7 +272,8 @@ int aphid_gpu_create(aphid_ctx **out, const aphid_opts *opts) {
     ctx->own_stream = true;
   }
   if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
-      cudaMallocHost(&ctx->h_done, sizeof(int)) != cudaSuccess) {
+      cudaMallocHost(&ctx->h_done, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_ndone, sizeof(int)) != cudaSuccess) {
     delete ctx;
     return APHID_ERR_CUDA;
   }
@@ -245,7 +287,12 @@ int aphid_gpu_destroy(aphid_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   release_work(ctx);
   cudaFree(ctx->d_tab);
+  cudaFree(ctx->d_sig);
+  cudaFree(ctx->d_epsr);
+  cudaFree(ctx->d_sig32);
+  cudaFree(ctx->d_epsr32);
   if (ctx->h_done) cudaFreeHost(ctx->h_done);
+  if (ctx->h_ndone) cudaFreeHost(ctx->h_ndone);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -274,11 +321,21 @@ int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz, const double *dx,
   CK(cudaStreamSynchronize(ctx->stream));
   release_work(ctx);
   cudaFree(ctx->d_tab);
+  cudaFree(ctx->d_sig);
+  cudaFree(ctx->d_epsr);
+  cudaFree(ctx->d_sig32);
+  cudaFree(ctx->d_epsr32);
   ctx->d_tab = nullptr;
+  ctx->d_sig = nullptr;
+  ctx->d_epsr = nullptr;
+  ctx->d_sig32 = nullptr;
+  ctx->d_epsr32 = nullptr;
   ctx->has_mesh = false;
+  ctx->has_model = false;
 
   std::vector<double> all, one;
   size_t offs[3];
+  for (int a = 0; a < 3; a++) ctx->host_d[a].assign(ds[a], ds[a] + dims[a] + 1);
   for (int a = 0; a < 3; a++) {
     axis_tables(dims[a], ds[a], dcs[a], one);
     offs[a] = all.size();
@@ -596,6 +653,403 @@ int aphid_gpu_fields(aphid_ctx *ctx, double omega, const aphid_z *a_x, const aph
   if ((rc = dl(e_x, e + ctx->g.ox, ctx->g.oy - ctx->g.ox)) || (rc = dl(e_y, e + ctx->g.oy, ctx->g.oz - ctx->g.oy)) ||
       (rc = dl(e_z, e + ctx->g.oz, ctx->g.op - ctx->g.oz)))
     return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return APHID_OK;
+}
+
+}  // extern "C"
+
+// ======================================================================
+// batched frequency sweep
+// ======================================================================
+namespace {
+
+SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
+  SweepDev D{};
+  D.g = ctx->g;
+  D.t = ctx->tiles;
+  D.tp = ctx->ptiles;
+  D.n = ctx->n;
+  D.nsys = nsys;
+  D.bps = ctx->sw_bps;
+  D.slots = ctx->sw_slots;
+  D.sig = ctx->d_sig;
+  D.epsr = ctx->d_epsr;
+  D.sig32 = ctx->d_sig32;
+  D.epsr32 = ctx->d_epsr32;
+  const size_t vec = (size_t)ctx->sw_nsys * ctx->n;
+  if (ctx->sw_f32_ok) {
+    D.v = ctx->sw_f32;
+    D.p = ctx->sw_f32 + vec;
+    D.q = ctx->sw_f32 + 2 * vec;
+    D.d = ctx->sw_f32 + 3 * vec;
+    D.x = ctx->sw_f32 + 4 * vec;
+    D.s = ctx->sw_f32 + 5 * vec;
+  }
+  D.x64 = ctx->sw_f64;
+  D.b = ctx->sw_f64 + vec;
+  D.sys = ctx->sw_sys;
+  D.part = ctx->sw_part;
+  D.cnt = ctx->sw_cnt;
+  D.ndone = ctx->sw_ndone;
+  return D;
+}
+
+int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
+  const bool grow = nsys > ctx->sw_nsys;
+  if (grow || (mixed && !ctx->sw_f32_ok)) {
+    if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+    ctx->sw_gexec = nullptr;
+  }
+  if (grow) {
+    cudaFree(ctx->sw_f64);
+    cudaFree(ctx->sw_f32);
+    cudaFree(ctx->sw_sys);
+    cudaFree(ctx->sw_part);
+    cudaFree(ctx->sw_cnt);
+    ctx->sw_f64 = nullptr;
+    ctx->sw_f32 = nullptr;
+    ctx->sw_f32_ok = false;
+    ctx->sw_nsys = 0;
+    const size_t vec = (size_t)nsys * ctx->n;
+    if (cudaMalloc(&ctx->sw_f64, 2 * vec * sizeof(double2)) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->sw_f64 = nullptr;
+      return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex128 vectors failed");
+    }
+    ctx->sw_bps = (int)std::max<long long>(
+        1, std::min<long long>((ctx->n + kStreamThreads - 1) / kStreamThreads, std::max(4, 148 * 8 / nsys)));
+    // plane tiles: about 4 waves of 148 SMs x 3 blocks over the whole batch
+    Tiles tp;
+    tp.ti = (ctx->nx + kPTI - 1) / kPTI;
+    tp.tj = (ctx->ny + kPTJ - 1) / kPTJ;
+    const long long cols = (long long)tp.ti * tp.tj * nsys;
+    tp.kz = (int)std::min<long long>(32, std::max<long long>(4, cols * ctx->nz / (148 * 3 * 4)));
+    tp.tk = (ctx->nz + tp.kz - 1) / tp.kz;
+    ctx->ptiles = tp;
+    ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()), tp.count());
+    CK(cudaMalloc(&ctx->sw_sys, (size_t)nsys * sizeof(SweepSys)));
+    CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * 6 * sizeof(double)));
+    CK(cudaMalloc(&ctx->sw_cnt, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
+    CK(cudaMemset(ctx->sw_cnt, 0, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
+    if (!ctx->sw_ndone) CK(cudaMalloc(&ctx->sw_ndone, sizeof(int)));
+    ctx->sw_nsys = nsys;
+  }
+  if (mixed && !ctx->sw_f32_ok) {
+    const size_t vec = (size_t)ctx->sw_nsys * ctx->n;
+    if (cudaMalloc(&ctx->sw_f32, 6 * vec * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->sw_f32 = nullptr;
+      return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex64 vectors failed");
+    }
+    ctx->sw_f32_ok = true;
+  }
+  return APHID_OK;
+}
+
+// oper_mode 5 sources (src/aphid.f90:638-741) as sparse (index, value) lists
+// per source, duplicates accumulated in file order.
+void source_entries(const aphid_ctx *ctx, int nsrc, const int *src_ndip, const char *dir, const int *ijk,
+                    std::vector<std::map<long long, double>> &out) {
+  const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+  const int lim[3] = {nx, ny, nz};
+  const long long off[3] = {ctx->g.ox, ctx->g.oy, ctx->g.oz};
+  out.assign(nsrc, {});
+  long long pos = 0;
+  for (int q = 0; q < nsrc; q++) {
+    for (int m = 0; m < src_ndip[q]; m++, pos++) {
+      const char s0 = dir[2 * pos], s1 = dir[2 * pos + 1];
+      if (!((s0 == '+' || s0 == '-') && (s1 == 'X' || s1 == 'Y' || s1 == 'Z'))) continue;
+      const int a = s1 - 'X';
+      int t[3] = {ijk[3 * pos] - 1, ijk[3 * pos + 1] - 1, ijk[3 * pos + 2] - 1};  // 0-based tail
+      if (s0 == '-') t[a] -= 1;  // "-X i j k" is the edge (i-1, i) with the opposite sign
+      bool ok = true;
+      for (int c = 0; c < 3; c++)
+        if (t[c] < 0 || t[c] > (c == a ? lim[c] - 2 : lim[c] - 1)) ok = false;
+      if (!ok) continue;
+      const double sgn = (s0 == '+') ? 1.0 : -1.0;
+      int h[3] = {t[0], t[1], t[2]};
+      h[a] += 1;
+      const int n1 = (a == 0) ? nx - 1 : nx, n2 = (a == 1) ? ny - 1 : ny;
+      const long long e = off[a] + t[0] + (long long)n1 * (t[1] + (long long)n2 * t[2]);
+      const long long pt = ctx->g.op + t[0] + (long long)nx * (t[1] + (long long)ny * t[2]);
+      const long long ph = ctx->g.op + h[0] + (long long)nx * (h[1] + (long long)ny * h[2]);
+      const double len = ctx->host_d[a][t[a] + 1];
+      out[q][e] += sgn * kMu0 * len;
+      out[q][pt] += sgn * kMu0;
+      out[q][ph] -= sgn * kMu0;
+    }
+  }
+}
+
+static __global__ void k_sw_scatter(long long cnt, const long long *__restrict__ idx,
+                                    const double *__restrict__ val, double2 *__restrict__ b) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < cnt) b[idx[t]] = make_double2(val[t], 0.0);
+}
+
+size_t apply_shm(const SweepDev &D) { return kApplyShm + (D.epsr32 ? kApplyShmEps : 0); }
+
+// opt in to the dynamic shared memory of the operator pass (once per context)
+int apply_attrs(aphid_ctx *ctx) {
+  const int bytes = (int)(kApplyShm + kApplyShmEps);
+  CK(cudaFuncSetAttribute(k_sw_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CK(cudaFuncSetAttribute(k_sw_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  return APHID_OK;
+}
+
+void sweep_round(aphid_ctx *ctx, const SweepDev &D) {
+  const unsigned ps = (unsigned)(D.bps * D.nsys);
+  const unsigned st = (unsigned)(D.t.count() * D.nsys);
+  const unsigned sp = (unsigned)(D.tp.count() * D.nsys);
+  k_sw_xupd<<<ps, kStreamThreads, 0, ctx->stream>>>(D);
+  k_sw_resid<<<st, kOpThreads, 0, ctx->stream>>>(D);
+  for (int it = 0; it < ctx->graph_iters; it++) {
+    k_sw_apply<true><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D);
+    k_sw_update<<<ps, kStreamThreads, 0, ctx->stream>>>(D);
+  }
+  k_sw_check<<<st, kOpThreads, 0, ctx->stream>>>(D);
+}
+
+int sweep_graph(aphid_ctx *ctx, const SweepDev &D) {
+  if (ctx->sw_gexec && ctx->sw_gkey == D.nsys) return APHID_OK;
+  int rc = apply_attrs(ctx);
+  if (rc) return rc;
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  sweep_round(ctx, D);
+  CK(cudaStreamEndCapture(ctx->stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&ctx->sw_gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate (sweep)");
+  ctx->sw_gkey = D.nsys;
+  return APHID_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, const float *eps_rel) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (csig_flag == 'D')
+    return fail(ctx, APHID_ERR_BADARG,
+                "Cole-Cole (D) is not linear in omega: use aphid_gpu_gen_k2 + aphid_gpu_qmr per frequency");
+  if (csig_flag != 'R' && csig_flag != 'C' && csig_flag != 'I')
+    return fail(ctx, APHID_ERR_BADARG, "csig_flag must be R, C or I");
+  if ((csig_flag != 'I' && !sig_re) || (csig_flag != 'R' && !eps_rel))
+    return fail(ctx, APHID_ERR_BADARG, "missing cell array for this conductivity model");
+  const long long ncell = (long long)(ctx->nx - 1) * (ctx->ny - 1) * (ctx->nz - 1);
+  // the captured sweep iteration holds the model pointers: drop it
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  ctx->has_model = false;
+  if (!ctx->d_sig) CK(cudaMalloc(&ctx->d_sig, ctx->n * sizeof(double)));
+  if (!ctx->d_sig32) CK(cudaMalloc(&ctx->d_sig32, ctx->n * sizeof(float)));
+  if (csig_flag != 'R') {
+    if (!ctx->d_epsr) CK(cudaMalloc(&ctx->d_epsr, ctx->n * sizeof(double)));
+    if (!ctx->d_epsr32) CK(cudaMalloc(&ctx->d_epsr32, ctx->n * sizeof(float)));
+  } else {
+    cudaFree(ctx->d_epsr);
+    cudaFree(ctx->d_epsr32);
+    ctx->d_epsr = nullptr;
+    ctx->d_epsr32 = nullptr;
+  }
+  float *cells = nullptr;
+  CK(cudaMalloc(&cells, ncell * sizeof(float)));
+  const dim3 grid = node_grid(ctx);
+  if (csig_flag == 'I') {
+    CK(cudaMemsetAsync(ctx->d_sig, 0, ctx->n * sizeof(double), ctx->stream));
+  } else {
+    CK(cudaMemcpyAsync(cells, sig_re, ncell * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    k_sw_avg<<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_sig);
+  }
+  if (csig_flag != 'R') {
+    CK(cudaMemcpyAsync(cells, eps_rel, ncell * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    k_sw_avg<<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_epsr);
+    k_sw_to32<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_epsr, ctx->d_epsr32);
+  }
+  k_sw_to32<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_sig, ctx->d_sig32);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(cells);
+  ctx->csig = csig_flag;
+  ctx->has_model = true;
+  return APHID_OK;
+}
+
+int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *source_of_system, int nsrc,
+                    const int *src_ndip, const char *dip_dir, const int *dip_ijk, const aphid_z *x0,
+                    const aphid_sweep_opts *opts, aphid_z *x_out, aphid_info *info) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->has_model) return fail(ctx, APHID_ERR_STATE, "aphid_gpu_set_model has not been called");
+  if (nsys < 1 || nsrc < 1 || !omega || !source_of_system || !src_ndip || !opts || !info)
+    return fail(ctx, APHID_ERR_BADARG, "sweep: bad counts or null arrays");
+  long long ndip = 0;
+  for (int q = 0; q < nsrc; q++) {
+    if (src_ndip[q] < 0) return fail(ctx, APHID_ERR_BADARG, "negative dipole count");
+    ndip += src_ndip[q];
+  }
+  if (ndip > 0 && (!dip_dir || !dip_ijk)) return fail(ctx, APHID_ERR_BADARG, "null dipole arrays");
+  for (int s = 0; s < nsys; s++) {
+    if (source_of_system[s] < 0 || source_of_system[s] >= nsrc)
+      return fail(ctx, APHID_ERR_BADARG, "source index out of range");
+    if (!std::isfinite(omega[s])) return fail(ctx, APHID_ERR_BADARG, "non-finite omega");
+  }
+  const bool mixed = opts->precision == APHID_PREC_MIXED;
+  if (!mixed && opts->precision != APHID_PREC_FP64) return fail(ctx, APHID_ERR_BADARG, "unknown precision");
+  if (!(opts->target >= 0.0) || opts->max_it < 0) return fail(ctx, APHID_ERR_BADARG, "bad target or max_it");
+  if (mixed && ctx->n >= (1LL << 31))
+    return fail(ctx, APHID_ERR_BADARG, "mixed sweep: more than 2^31 unknowns per system");
+  if (mixed && (long long)ctx->nz * nsys > 65535)
+    return fail(ctx, APHID_ERR_BADARG, "nz * nsys exceeds the launch grid; split the sweep");
+  if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
+  if ((rc = ensure_work(ctx))) return rc;
+
+  // sources -> sparse right-hand sides
+  std::vector<std::map<long long, double>> src;
+  source_entries(ctx, nsrc, src_ndip, dip_dir, dip_ijk, src);
+  std::vector<long long> eidx;
+  std::vector<double> eval;
+  for (int s = 0; s < nsys; s++)
+    for (const auto &kv : src[source_of_system[s]]) {
+      eidx.push_back((long long)s * ctx->n + kv.first);
+      eval.push_back(kv.second);
+    }
+  SweepDev D = sweep_dev(ctx, nsys);
+  const size_t vec = (size_t)nsys * ctx->n;
+  double2 *b = D.b, *x64 = D.x64;
+  long long *d_idx = nullptr;
+  double *d_val = nullptr;
+  CK(cudaMemsetAsync(b, 0, vec * sizeof(double2), ctx->stream));
+  if (!eidx.empty()) {
+    CK(cudaMalloc(&d_idx, eidx.size() * sizeof(long long)));
+    CK(cudaMalloc(&d_val, eval.size() * sizeof(double)));
+    CK(cudaMemcpyAsync(d_idx, eidx.data(), eidx.size() * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_val, eval.data(), eval.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    k_sw_scatter<<<(unsigned)((eidx.size() + 255) / 256), 256, 0, ctx->stream>>>((long long)eidx.size(), d_idx,
+                                                                                 d_val, b);
+  }
+  if (x0)
+    CK(cudaMemcpyAsync(x64, x0, vec * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  else
+    CK(cudaMemsetAsync(x64, 0, vec * sizeof(double2), ctx->stream));
+
+  std::vector<SweepSys> hs(nsys);
+  for (int s = 0; s < nsys; s++) {
+    SweepSys &S = hs[s];
+    S = SweepSys{};
+    S.omega = omega[s];
+    S.ka = omega[s] * omega[s] * kMu0 * kEps0;
+    S.kb = omega[s] * kMu0;
+    S.target = opts->target;
+    S.max_it = opts->max_it;
+    S.inner_tol = opts->inner_tol > 0 ? opts->inner_tol : 1e-10;
+    S.max_outer = opts->max_outer > 0 ? opts->max_outer : 40;
+    S.phase = PH_OUTER;
+    S.status = -1;
+  }
+  CK(cudaMemcpyAsync(ctx->sw_sys, hs.data(), nsys * sizeof(SweepSys), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->sw_ndone, 0, sizeof(int), ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  long long nlaunch = 0;
+  std::vector<aphid_info> out(nsys);
+
+  if (mixed) {
+    k_sw_bnorm<<<(unsigned)(D.bps * nsys), kStreamThreads, 0, ctx->stream>>>(D);
+    const dim3 sg((unsigned)((ctx->nx + 127) / 128), (unsigned)ctx->ny, (unsigned)(ctx->nz * nsys));
+    k_sw_scale<<<sg, 128, 0, ctx->stream>>>(D);
+    CK(cudaGetLastError());
+    nlaunch += 2;
+    if ((rc = sweep_graph(ctx, D))) return rc;
+    const long long per_round = 3 + 2LL * ctx->graph_iters;
+    const long long max_rounds = (long long)std::max(1, opts->max_it) / ctx->graph_iters + 2LL * (hs[0].max_outer + 2);
+    for (long long round = 0;; round++) {
+      CK(cudaMemcpyAsync(ctx->h_ndone, ctx->sw_ndone, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (*ctx->h_ndone >= nsys) break;
+      if (round > max_rounds) return fail(ctx, APHID_ERR_STATE, "sweep did not terminate");
+      CK(cudaGraphLaunch(ctx->sw_gexec, ctx->stream));
+      nlaunch += per_round;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaMemcpyAsync(hs.data(), ctx->sw_sys, nsys * sizeof(SweepSys), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int s = 0; s < nsys; s++) {
+      const SweepSys &S = hs[s];
+      aphid_info &I = out[s];
+      I.status = S.status;
+      I.iters = S.total_it;
+      I.inner_iters = S.total_it;
+      I.outer_iters = S.outer_it;
+      I.rhs_norm = S.bnorm;
+      I.recur_resid = S.tau;
+      I.true_rel_resid = S.bnorm > 0 ? S.rnorm / S.bnorm : S.rnorm;
+    }
+  } else {
+    // the reference's own algorithm, one system at a time, on resident data
+    double2 *k2 = wv(ctx, W_K2), *dg = wv(ctx, W_INV);
+    for (int s = 0; s < nsys; s++) {
+      k_sw_k2vec<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_sig, ctx->d_epsr, hs[s].ka,
+                                                                 hs[s].kb, k2);
+      k_gen_diag<<<node_grid(ctx), 128, 0, ctx->stream>>>(ctx->g, k2, dg);
+      CK(cudaMemcpyAsync(wv(ctx, W_B), b + (size_t)s * ctx->n, ctx->n * sizeof(double2),
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(wv(ctx, W_X), x64 + (size_t)s * ctx->n, ctx->n * sizeof(double2),
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+      ctx->loaded = true;
+      ctx->inv_ready = false;
+      aphid_info I{};
+      if ((rc = qmr_run(ctx, opts->target, opts->max_it, x0 != nullptr, nullptr, 0, &I))) return rc;
+      CK(cudaMemcpyAsync(x64 + (size_t)s * ctx->n, wv(ctx, W_X), ctx->n * sizeof(double2),
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+      nlaunch += 2 + I.kernel_launches;
+      out[s] = I;
+    }
+    ctx->loaded = false;
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  cudaFree(d_idx);
+  cudaFree(d_val);
+  for (int s = 0; s < nsys; s++) {
+    out[s].seconds = ms * 1e-3;
+    out[s].kernel_launches = nlaunch;
+    info[s] = out[s];
+  }
+  ctx->sw_last = nsys;
+  if (x_out) {
+    CK(cudaMemcpyAsync(x_out, x64, vec * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return APHID_OK;
+}
+
+int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (ctx->sw_last < 1 || !ctx->sw_f32_ok || reps < 1)
+    return fail(ctx, APHID_ERR_STATE, "no complex64 sweep state on the device");
+  const SweepDev D = sweep_dev(ctx, ctx->sw_last);
+  const unsigned sp = (unsigned)(D.tp.count() * D.nsys);
+  if ((rc = apply_attrs(ctx))) return rc;
+  for (int r = 0; r < reps; r++) k_sw_apply<false><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D);
+  CK(cudaGetLastError());
+  return APHID_OK;
+}
+
+int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (sys < 0 || sys >= ctx->sw_last || !x) return fail(ctx, APHID_ERR_BADARG, "no such system in the last sweep");
+  CK(cudaMemcpyAsync(x, ctx->sw_f64 + (size_t)sys * ctx->n, ctx->n * sizeof(double2), cudaMemcpyDeviceToHost,
+                     ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return APHID_OK;
 }

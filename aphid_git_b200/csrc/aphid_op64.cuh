@@ -21,7 +21,7 @@ constexpr int kTileI = 32, kTileJ = 4, kOpThreads = kTileI * kTileJ;
 
 struct Tiles {
   int ti, tj, tk, kz;
-  long long count() const { return (long long)ti * tj * tk; }
+  __host__ __device__ long long count() const { return (long long)ti * tj * tk; }
 };
 
 __device__ __forceinline__ void tile_coords(const Tiles &t, int &i, int &j, int &k0, int &k1, int nz) {

@@ -176,6 +176,38 @@ def only_apply(s, k2, n, dev, stream):
     return 0
 
 
+def timed(stream, dev, fn, steps, barrier, world):
+    """Run fn() `steps` times between CUDA events on `stream`, barrier and
+    synchronize on both sides; returns (ms max over ranks, results)."""
+    import torch
+    import torch.distributed as dist
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = [fn() for _ in range(steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, out
+
+
+def systems_of(m):
+    """(omega, source index) of every system, frequencies fastest, as the
+    reference's MPI farm orders them (src/aphid_parallel.f90:97-101)."""
+    om, sos = [], []
+    for q in range(len(m.sources)):
+        for f in m.freqs:
+            om.append(2 * np.pi * float(f))
+            sos.append(q)
+    return om, sos
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -183,7 +215,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hetero96")
-    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--inner-tol", type=float, default=0.0)
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="timed complex128 solves for the speed-up comparison (0: skip)")
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only-apply", action="store_true",
@@ -201,13 +236,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
     if world > 1:
         import datetime
-        torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     # a real stream (not the NULL stream) shared by the library and the
     # CUDA events, so the events bracket the library's kernels
@@ -221,98 +254,142 @@ def main():
     m, w, sig, b = setup_problem(args.workload)
     s = Solver(device=local, stream=stream.cuda_stream)
     s.set_nodes(m.xn, m.yn, m.zn)
-    k2 = s.gen_k2(sig, w)
-    diag = s.gen_diag(k2)
     n = s.n
-
-    if args.only_apply:
-        return only_apply(s, k2, n, dev, stream)
-
-    # ---- resident solve: value
-    s.qmr_load(k2, diag, b)
-    for _ in range(args.warmup):
-        info, _ = s.qmr_run(TARGET, MAX_IT)
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
-    barrier()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    infos = []
-    for _ in range(args.steps):
-        info, _ = s.qmr_run(TARGET, MAX_IT)
-        infos.append(info)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    iters = infos[-1]["iters"]
-    sweeps = world * args.steps
-    value = sweeps / (ms * 1e-3)
-    launches = int(sum(i["kernel_launches"] for i in infos))
-
-    # ---- public host-buffer call: e2e
-    barrier()
-    torch.cuda.synchronize(dev)
-    e0.record(stream)
-    for _ in range(args.steps):
-        x, info_e, _ = s.qmr(k2, diag, b, TARGET, MAX_IT, hist=False)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    ms_e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e = float(t.item())
-    e2e = {"value": sweeps / (ms_e * 1e-3), "unit": "sweeps/s",
-           "h2d_bytes_per_step": 3 * 16 * n, "d2h_bytes_per_step": 16 * n}
-
-    # ---- roofline of the dominant kernel: the operator apply of a QMR step
-    # (q = K p with epsilon = p^T q reduced in the same pass), timed alone on
-    # the library's stream with CUDA events.  Algorithmic bytes per launch:
-    # read p and k^2, write q: 3 x 16 B per unknown.
-    t_apply = time_apply(s, k2, n, dev, stream)
+    om, sos = systems_of(m)
+    nsys = len(om)
     peak, peak_kind = peaks()
-    alg = 3 * 16 * n
+    clocks = ClockSampler(local)
+
+    if args.only_apply and args.precision == "mixed":
+        # resident complex64 state from a short sweep, then the operator pass
+        s.set_model("R", m.sig_re)
+        s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=8, fetch=False)
+        ms_a, _ = timed(stream, dev, lambda: s.sweep_time_apply(10), 1, lambda: None, 1)
+        t = ms_a * 1e-3 / 10
+        print(json.dumps({"apply_us": t * 1e6, "unknowns": n, "systems": nsys,
+                          "alg_GBps": (nsys * n * 32 + n * 8) / t / 1e9}))
+        return 0
+
+    plain = None
+    if args.precision == "fp64" or args.only_apply or args.plain_steps > 0:
+        # the plain complex128 path: the reference's algorithm, one system at
+        # a time, inputs resident (k^2, Jacobi diagonal and b on the device)
+        k2 = s.gen_k2(sig, w)
+        diag = s.gen_diag(k2)
+        if args.only_apply:
+            return only_apply(s, k2, n, dev, stream)
+        s.qmr_load(k2, diag, b)
+        s.qmr_run(TARGET, MAX_IT)
+        steps = args.steps if args.precision == "fp64" else args.plain_steps
+        if args.precision == "fp64":
+            for _ in range(args.warmup - 1):
+                s.qmr_run(TARGET, MAX_IT)
+            clocks.start()
+            time.sleep(0.3)
+        ms_p, inf_p = timed(stream, dev, lambda: s.qmr_run(TARGET, MAX_IT)[0], steps, barrier, world)
+        plain = {"time_to_tol_s": ms_p / steps * 1e-3, "iters_to_tol": inf_p[-1]["iters"],
+                 "true_rel_resid": inf_p[-1]["true_rel_resid"],
+                 "launches": int(sum(i["kernel_launches"] for i in inf_p)), "ms": ms_p,
+                 "steps": steps, "note": "complex128 Jacobi-QMR, reference recurrence, "
+                 "first system of the workload"}
+
+    if args.precision == "fp64":
+        clk = clocks.stop()
+        ms, launches = plain["ms"], plain["launches"]
+        iters = plain["iters_to_tol"]
+        value = world * args.steps / (ms * 1e-3)
+        ms_e, _ = timed(stream, dev, lambda: s.qmr(k2, diag, b, TARGET, MAX_IT, hist=False)[1],
+                        args.steps, barrier, world)
+        e2e = {"value": world * args.steps / (ms_e * 1e-3), "unit": "sweeps/s",
+               "h2d_bytes_per_step": 3 * 16 * n, "d2h_bytes_per_step": 16 * n}
+        t_apply = time_apply(s, k2, n, dev, stream)
+        alg = 3 * 16 * n
+        kernel = "k_apply64 (complex128 QMR step: q = K p, epsilon)"
+        extra = {"time_to_tol_s": ms / args.steps * 1e-3, "iters_to_tol": iters,
+                 "qmr_iters_per_s": world * args.steps * iters / (ms * 1e-3),
+                 "true_rel_resid": plain["true_rel_resid"]}
+        dtype = "c128"
+        traffic_key = "apply64_qmr_" + args.workload
+    else:
+        # the product path: batched mixed-precision sweep of all systems
+        s.set_model("R", m.sig_re)
+
+        def run_sweep():
+            return s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=MAX_IT,
+                           inner_tol=args.inner_tol, fetch=False)[1]
+
+        for _ in range(args.warmup):
+            run_sweep()
+        clocks.start()
+        time.sleep(0.3)
+        ms, infs = timed(stream, dev, run_sweep, args.steps, barrier, world)
+        clk = clocks.stop()
+        last = infs[-1]
+        launches = int(sum(i[0]["kernel_launches"] for i in infs))
+        value = world * args.steps / (ms * 1e-3)
+
+        def run_e2e():
+            s.set_model("R", m.sig_re)
+            return s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=MAX_IT,
+                           inner_tol=args.inner_tol, fetch=True)[1]
+
+        ms_e, _ = timed(stream, dev, run_e2e, args.steps, barrier, world)
+        e2e = {"value": world * args.steps / (ms_e * 1e-3), "unit": "sweeps/s",
+               "h2d_bytes_per_step": 4 * m.ncell, "d2h_bytes_per_step": 16 * n * nsys}
+        # dominant kernel: the complex64 operator pass of the inner QMR.
+        # Algorithmic bytes per launch: per system read v~, p~, D^-1/2 and
+        # write q~ (4 x 8 B per unknown), plus the shared FP64 sigma-bar once.
+        reps = 20
+        s.sweep_time_apply(3)
+        ms_a, _ = timed(stream, dev, lambda: s.sweep_time_apply(reps), 1, lambda: None, 1)
+        t_apply = ms_a * 1e-3 / reps
+        alg = nsys * n * 32 + n * 8
+        kernel = "k_sw_apply (complex64 operator pass: q~ = D^-1/2 K D^-1/2 p~, 6 sums)"
+        it_in = [i["inner_iters"] for i in last]
+        extra = {"time_to_tol_s": ms / args.steps * 1e-3, "systems": nsys,
+                 "inner_iters_max": max(it_in), "inner_iters_total": int(sum(it_in)),
+                 "outer_iters_max": max(i["outer_iters"] for i in last),
+                 "qmr_iters_per_s": world * args.steps * sum(it_in) / (ms * 1e-3),
+                 "true_rel_resid_max": max(i["true_rel_resid"] for i in last),
+                 "status": sorted({i["status_name"] for i in last})}
+        if plain is not None:
+            extra["plain_fp64"] = plain
+            extra["speedup_vs_plain_fp64"] = plain["time_to_tol_s"] * nsys / (ms / args.steps * 1e-3)
+        dtype = "c64 inner / f64 outer"
+        traffic_key = "sw_apply_" + args.workload
+
     achieved = alg / t_apply / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get("apply64_qmr_" + args.workload)
-
+            traffic = json.load(f).get(traffic_key)
     line = {
         "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
         "data": "synthetic (seeded generator, no public dataset)",
         "config": {"workload": args.workload, "precision": args.precision, "unknowns": n,
-                   "target": TARGET, "l2": "working set > L2 (126 MB), no flush",
+                   "systems": nsys, "target": TARGET,
+                   "l2": "working set > L2 (126 MB), no flush",
                    "parallelism": "independent sweep per GPU"},
-        "time_to_tol_s": ms / args.steps * 1e-3, "iters_to_tol": iters,
-        "qmr_iters_per_s": world * args.steps * iters / (ms * 1e-3),
-        "true_rel_resid": infos[-1]["true_rel_resid"], "status": infos[-1]["status_name"],
         "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-        "roofline": {"bound": "hbm", "kernel": "k_apply64 (QMR step)", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
                      "traffic": traffic, "alg_bytes_per_launch": alg,
                      "launch_us": t_apply * 1e6},
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    line.update(extra)
+    iters_ref = FP64_ITERS.get(args.workload)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and iters_ref:
         spi, done = cpu_port_sample(args.workload, args.cpu_sample_iters)
         line["cpu_baseline"] = {
-            "value": 1.0 / (spi * iters), "unit": "sweeps/s", "cores": 4, "kind": "port",
+            "value": 1.0 / (spi * iters_ref * nsys), "unit": "sweeps/s", "cores": 4,
+            "kind": "port",
             "sample": "%d QMR iterations of the workload, oracle 4-thread component split; "
-                      "time-to-tolerance = %.3f s/iter x %d iterations (GPU count, same recurrence)"
-                      % (done, spi, iters),
+                      "time-to-tolerance = %.3f s/iter x %d iterations (complex128 count, same "
+                      "recurrence) x %d systems" % (done, spi, iters_ref, nsys),
             "s_per_iter": spi}
     s.close()
     if rank == 0:

@@ -176,6 +176,59 @@ int aphid_gpu_qmr_fetch(aphid_ctx *ctx, aphid_z *sol_x, aphid_z *sol_y,
 int aphid_gpu_inprod_dev(aphid_ctx *ctx, const void *d_k2, const void *d_in,
                          void *d_out, void *d_eps);
 
+/* ---- batched frequency sweep ------------------------------------------- */
+
+/* Cell model for the sweep: csig_flag 'R' (sig_re; sigma-hat = sigma +
+ * i omega eps0), 'C' (sig_re and eps_rel; sigma + i omega eps0 eps_rel) or
+ * 'I' (eps_rel only; i omega eps0 eps_rel), the linear models of read_mesh
+ * (src/aphid.f90:379-449), real(4) cell arrays (nx-1,ny-1,nz-1).  The
+ * area/volume-weighted averages of gen_k2_*grid are formed once on the device
+ * in FP64; every system's k^2 follows from them and its omega.  'D'
+ * (Cole-Cole) is not linear in omega and is rejected here: use
+ * aphid_gpu_gen_k2 + aphid_gpu_qmr per frequency. */
+int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re,
+                        const float *eps_rel);
+
+typedef struct {
+  int precision;      /* APHID_PREC_MIXED or APHID_PREC_FP64 */
+  double target;      /* MIXED: stop when ||b - K x||_2 < target ||b||_2 (FP64
+                         true residual); FP64: the reference's recurrence
+                         stop test with this qmr_target */
+  int max_it;         /* iteration cap per system (inner iterations, MIXED) */
+  double inner_tol;   /* MIXED: cap on the inner quasi-residual reduction per
+                         defect-correction step (0 = 1e-10); a cycle also
+                         ends when the true residual, checked every graph
+                         round, converges or stagnates */
+  int max_outer;      /* MIXED: cap on defect-correction steps (0 = 40) */
+  int reserved[3];
+} aphid_sweep_opts;
+
+/* Solve nsys systems (frequency x source) on the context's mesh and model:
+ * the MPI farm of src/aphid_parallel.f90 as one batched GPU solve.  System s
+ * has angular frequency omega[s] and source source_of_system[s]; source q is
+ * an oper_mode-5 dipole list (src/aphid.f90:638-741) of src_ndip[q] dipoles,
+ * stored consecutively in dip_dir (2 chars each, "+X" ... "-Z") and dip_ijk
+ * (1-based tail-end node, 3 ints each).  Out-of-range or invalid dipoles are
+ * skipped, as the reference does.
+ * x0 (nullable): nsys concatenated [x|y|z|p] initial guesses.
+ * x_out (nullable): nsys concatenated solutions; when NULL the solutions stay
+ * on the device for aphid_gpu_sweep_fetch.  info: nsys records. */
+int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega,
+                    const int *source_of_system, int nsrc, const int *src_ndip,
+                    const char *dip_dir, const int *dip_ijk, const aphid_z *x0,
+                    const aphid_sweep_opts *opts, aphid_z *x_out,
+                    aphid_info *info);
+
+/* Copy system `sys` of the last sweep into x (one [x|y|z|p] vector). */
+int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);
+
+/* Benchmarking hook, no counterpart in the reference: launch the complex64
+ * operator pass of the inner QMR (q~ = D^-1/2 K D^-1/2 p~ with its epsilon
+ * and rho sums) `reps` times over all systems of the last mixed-precision
+ * sweep, on the context's stream, without the scalar recurrence, so no system
+ * changes state.  Returns after the launches (asynchronous). */
+int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps);
+
 /* ---- allocation-free operator apply -------------------------------------- */
 
 /* No counterpart in the reference: an addition for callers that cannot call
