@@ -33,7 +33,7 @@ class SweepOpts(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("stream", C.c_void_p), ("graph_iters", C.c_int),
-                ("verbose", C.c_int)]
+                ("verbose", C.c_int), ("plane_kz", C.c_int)]
 
 
 class Info(C.Structure):
@@ -128,10 +128,10 @@ def inprod_eps_noalloc(nx, ny, nz, d_spacing, d_k2, d_in, d_out, d_eps, stream=0
 class Solver:
     """One GPU context (one per host thread), bound to a mesh."""
 
-    def __init__(self, device=0, stream=None, graph_iters=0, verbose=False):
+    def __init__(self, device=0, stream=None, graph_iters=0, verbose=False, plane_kz=0):
         self.lib = load()
         self._h = C.c_void_p()
-        o = Opts(device, stream or 0, graph_iters, int(verbose))
+        o = Opts(device, stream or 0, graph_iters, int(verbose), plane_kz)
         rc = self.lib.aphid_gpu_create(C.byref(self._h), C.byref(o))
         if rc != APHID_OK:
             raise AphidError("aphid_gpu_create failed: %s" % ERRORS.get(rc, rc))

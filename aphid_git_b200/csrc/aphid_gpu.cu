@@ -25,6 +25,7 @@ struct aphid_ctx {
   bool own_stream = false;
   int graph_iters = 16;
   int verbose = 0;
+  int plane_kz = 0;
   std::string err;
 
   // mesh
@@ -36,6 +37,7 @@ struct aphid_ctx {
   GridDev g{};
   Tiles tiles{};
   Tiles ptiles{};  // plane tiles of the complex64 operator pass
+  NodeLayout nl{};  // node layout of the complex64 sweep state
   int sblk = 0;  // blocks of the streaming kernels
 
   // complex128 work space: k2 inv b x r s p d v q
@@ -66,7 +68,9 @@ struct aphid_ctx {
   int sw_nsys = 0;           // systems the buffers hold
   bool sw_f32_ok = false;    // complex64 vectors allocated
   double2 *sw_f64 = nullptr; // [2][nsys][n]: x64, b
-  float2 *sw_f32 = nullptr;  // [6][nsys][n]: v p q d x s
+  float2 *sw_f32 = nullptr;  // [6][nsys][4][N]: v p q d x s (node layout)
+  ApplyMaps maps{};          // TMA tensor maps of the operator pass
+  int *sw_err = nullptr;     // set by a kernel whose bounded wait gave up
   SweepSys *sw_sys = nullptr;
   double *sw_part = nullptr;
   unsigned *sw_cnt = nullptr;
@@ -137,6 +141,8 @@ void release_work(aphid_ctx *ctx) {
   cudaFree(ctx->sw_part);
   cudaFree(ctx->sw_cnt);
   cudaFree(ctx->sw_ndone);
+  cudaFree(ctx->sw_err);
+  ctx->sw_err = nullptr;
   ctx->sw_f64 = nullptr;
   ctx->sw_f32 = nullptr;
   ctx->sw_sys = nullptr;
@@ -247,6 +253,7 @@ int aphid_gpu_create(aphid_ctx **out, const aphid_opts *opts) {
     ctx->stream = (cudaStream_t)opts->stream;
     if (opts->graph_iters > 0) ctx->graph_iters = std::min(opts->graph_iters, 256);
     ctx->verbose = opts->verbose;
+    if (opts->plane_kz > 0) ctx->plane_kz = std::min(opts->plane_kz, 256);
   }
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -375,6 +382,8 @@ int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz, const double *dx,
   t.kz = (int)std::min<long long>(32, std::max<long long>(1, cols * nz / (148 * 8)));
   t.tk = (nz + t.kz - 1) / t.kz;
   ctx->tiles = t;
+  ctx->nl.nxp = (nx + 3) / 4 * 4;
+  ctx->nl.N = (long long)ctx->nl.nxp * ny * nz;
   ctx->sblk = (int)std::max<long long>(1, std::min<long long>((n + kStreamThreads - 1) / kStreamThreads, 148 * 8));
   ctx->has_mesh = true;
   return APHID_OK;
@@ -664,6 +673,62 @@ int aphid_gpu_fields(aphid_ctx *ctx, double omega, const aphid_z *a_x, const aph
 // ======================================================================
 namespace {
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_map(aphid_ctx *ctx, CUtensorMap *m, CUtensorMapDataType type, int rank, void *base,
+               const cuuint64_t *dims, const cuuint64_t *strides, const cuuint32_t *box) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess || !f)
+      return fail(ctx, APHID_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = (EncodeTiledFn)f;
+  }
+  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  const CUresult r = fn(m, type, (cuuint32_t)rank, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, APHID_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return APHID_OK;
+}
+
+// v~, p~, D^-1/2: 5-D (i, j, k, component, system) over 8-byte elements, one
+// box = 20 x 18 nodes of one z-plane, all four components
+int vector_maps(aphid_ctx *ctx) {
+  const NodeLayout &L = ctx->nl;
+  const size_t v32 = (size_t)ctx->sw_nsys * 4 * L.N;
+  const cuuint64_t dims[5] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4,
+                              (cuuint64_t)ctx->sw_nsys};
+  const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * 8, (cuuint64_t)L.nxp * ctx->ny * 8, (cuuint64_t)L.N * 8,
+                                 (cuuint64_t)L.N * 32};
+  const cuuint32_t box[5] = {kPW, kPH, 1, 4, 1};
+  int rc;
+  if ((rc = encode_map(ctx, &ctx->maps.v, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32, dims, strides, box)))
+    return rc;
+  if ((rc = encode_map(ctx, &ctx->maps.p, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + v32, dims, strides, box)))
+    return rc;
+  return encode_map(ctx, &ctx->maps.s, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + 5 * v32, dims, strides, box);
+}
+
+// sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18
+int model_maps(aphid_ctx *ctx) {
+  const NodeLayout &L = ctx->nl;
+  const cuuint64_t dims[4] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4};
+  const cuuint64_t strides[3] = {(cuuint64_t)L.nxp * 4, (cuuint64_t)L.nxp * ctx->ny * 4, (cuuint64_t)L.N * 4};
+  const cuuint32_t box[4] = {kKW, kPH, 1, 4};
+  int rc = encode_map(ctx, &ctx->maps.sig, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->d_sig32, dims, strides, box);
+  if (rc) return rc;
+  if (ctx->d_epsr32)
+    return encode_map(ctx, &ctx->maps.eps, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->d_epsr32, dims, strides, box);
+  ctx->maps.eps = ctx->maps.sig;  // unused without eps-bar
+  return APHID_OK;
+}
+
 SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   SweepDev D{};
   D.g = ctx->g;
@@ -677,14 +742,17 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   D.epsr = ctx->d_epsr;
   D.sig32 = ctx->d_sig32;
   D.epsr32 = ctx->d_epsr32;
+  D.L = ctx->nl;
+  D.err = ctx->sw_err;
   const size_t vec = (size_t)ctx->sw_nsys * ctx->n;
+  const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
   if (ctx->sw_f32_ok) {
     D.v = ctx->sw_f32;
-    D.p = ctx->sw_f32 + vec;
-    D.q = ctx->sw_f32 + 2 * vec;
-    D.d = ctx->sw_f32 + 3 * vec;
-    D.x = ctx->sw_f32 + 4 * vec;
-    D.s = ctx->sw_f32 + 5 * vec;
+    D.p = ctx->sw_f32 + v32;
+    D.q = ctx->sw_f32 + 2 * v32;
+    D.d = ctx->sw_f32 + 3 * v32;
+    D.x = ctx->sw_f32 + 4 * v32;
+    D.s = ctx->sw_f32 + 5 * v32;
   }
   D.x64 = ctx->sw_f64;
   D.b = ctx->sw_f64 + vec;
@@ -724,7 +792,9 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     tp.ti = (ctx->nx + kPTI - 1) / kPTI;
     tp.tj = (ctx->ny + kPTJ - 1) / kPTJ;
     const long long cols = (long long)tp.ti * tp.tj * nsys;
-    tp.kz = (int)std::min<long long>(32, std::max<long long>(4, cols * ctx->nz / (148 * 3 * 4)));
+    tp.kz = ctx->plane_kz > 0
+                ? ctx->plane_kz
+                : (int)std::min<long long>(32, std::max<long long>(8, cols * ctx->nz / (148 * 3 * 2)));
     tp.tk = (ctx->nz + tp.kz - 1) / tp.kz;
     ctx->ptiles = tp;
     ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()), tp.count());
@@ -736,13 +806,18 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     ctx->sw_nsys = nsys;
   }
   if (mixed && !ctx->sw_f32_ok) {
-    const size_t vec = (size_t)ctx->sw_nsys * ctx->n;
-    if (cudaMalloc(&ctx->sw_f32, 6 * vec * sizeof(float2)) != cudaSuccess) {
+    const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
+    if (cudaMalloc(&ctx->sw_f32, 6 * v32 * sizeof(float2)) != cudaSuccess) {
       cudaGetLastError();
       ctx->sw_f32 = nullptr;
       return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex64 vectors failed");
     }
+    // pads and components that do not exist stay zero for good
+    CK(cudaMemset(ctx->sw_f32, 0, 6 * v32 * sizeof(float2)));
+    if (!ctx->sw_err) CK(cudaMalloc(&ctx->sw_err, sizeof(int)));
     ctx->sw_f32_ok = true;
+    int rc = vector_maps(ctx);
+    if (rc) return rc;
   }
   return APHID_OK;
 }
@@ -805,7 +880,7 @@ void sweep_round(aphid_ctx *ctx, const SweepDev &D) {
   k_sw_xupd<<<ps, kStreamThreads, 0, ctx->stream>>>(D);
   k_sw_resid<<<st, kOpThreads, 0, ctx->stream>>>(D);
   for (int it = 0; it < ctx->graph_iters; it++) {
-    k_sw_apply<true><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D);
+    k_sw_apply<true><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D, ctx->maps);
     k_sw_update<<<ps, kStreamThreads, 0, ctx->stream>>>(D);
   }
   k_sw_check<<<st, kOpThreads, 0, ctx->stream>>>(D);
@@ -848,10 +923,10 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
   ctx->sw_gexec = nullptr;
   ctx->has_model = false;
   if (!ctx->d_sig) CK(cudaMalloc(&ctx->d_sig, ctx->n * sizeof(double)));
-  if (!ctx->d_sig32) CK(cudaMalloc(&ctx->d_sig32, ctx->n * sizeof(float)));
+  if (!ctx->d_sig32) CK(cudaMalloc(&ctx->d_sig32, 4 * ctx->nl.N * sizeof(float)));
   if (csig_flag != 'R') {
     if (!ctx->d_epsr) CK(cudaMalloc(&ctx->d_epsr, ctx->n * sizeof(double)));
-    if (!ctx->d_epsr32) CK(cudaMalloc(&ctx->d_epsr32, ctx->n * sizeof(float)));
+    if (!ctx->d_epsr32) CK(cudaMalloc(&ctx->d_epsr32, 4 * ctx->nl.N * sizeof(float)));
   } else {
     cudaFree(ctx->d_epsr);
     cudaFree(ctx->d_epsr32);
@@ -870,12 +945,15 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
   if (csig_flag != 'R') {
     CK(cudaMemcpyAsync(cells, eps_rel, ncell * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     k_sw_avg<<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_epsr);
-    k_sw_to32<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_epsr, ctx->d_epsr32);
+    CK(cudaMemsetAsync(ctx->d_epsr32, 0, 4 * ctx->nl.N * sizeof(float), ctx->stream));
+    k_sw_to_node32<<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_epsr, ctx->d_epsr32);
   }
-  k_sw_to32<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_sig, ctx->d_sig32);
+  CK(cudaMemsetAsync(ctx->d_sig32, 0, 4 * ctx->nl.N * sizeof(float), ctx->stream));
+  k_sw_to_node32<<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_sig, ctx->d_sig32);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   cudaFree(cells);
+  if ((rc = model_maps(ctx))) return rc;
   ctx->csig = csig_flag;
   ctx->has_model = true;
   return APHID_OK;
@@ -903,8 +981,8 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
   const bool mixed = opts->precision == APHID_PREC_MIXED;
   if (!mixed && opts->precision != APHID_PREC_FP64) return fail(ctx, APHID_ERR_BADARG, "unknown precision");
   if (!(opts->target >= 0.0) || opts->max_it < 0) return fail(ctx, APHID_ERR_BADARG, "bad target or max_it");
-  if (mixed && ctx->n >= (1LL << 31))
-    return fail(ctx, APHID_ERR_BADARG, "mixed sweep: more than 2^31 unknowns per system");
+  if (mixed && 4 * ctx->nl.N >= (1LL << 31))
+    return fail(ctx, APHID_ERR_BADARG, "mixed sweep: more than 2^31 node-layout values per system");
   if (mixed && (long long)ctx->nz * nsys > 65535)
     return fail(ctx, APHID_ERR_BADARG, "nz * nsys exceeds the launch grid; split the sweep");
   if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
@@ -955,6 +1033,7 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
   }
   CK(cudaMemcpyAsync(ctx->sw_sys, hs.data(), nsys * sizeof(SweepSys), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->sw_ndone, 0, sizeof(int), ctx->stream));
+  if (mixed) CK(cudaMemsetAsync(ctx->sw_err, 0, sizeof(int), ctx->stream));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   long long nlaunch = 0;
   std::vector<aphid_info> out(nsys);
@@ -978,7 +1057,10 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     CK(cudaMemcpyAsync(hs.data(), ctx->sw_sys, nsys * sizeof(SweepSys), cudaMemcpyDeviceToHost, ctx->stream));
+    int kerr = 0;
+    CK(cudaMemcpyAsync(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (kerr) return fail(ctx, APHID_ERR_CUDA, "sweep: a tensor-copy wait in the operator pass timed out");
     for (int s = 0; s < nsys; s++) {
       const SweepSys &S = hs[s];
       aphid_info &I = out[s];
@@ -1039,7 +1121,7 @@ int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {
   const SweepDev D = sweep_dev(ctx, ctx->sw_last);
   const unsigned sp = (unsigned)(D.tp.count() * D.nsys);
   if ((rc = apply_attrs(ctx))) return rc;
-  for (int r = 0; r < reps; r++) k_sw_apply<false><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D);
+  for (int r = 0; r < reps; r++) k_sw_apply<false><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D, ctx->maps);
   CK(cudaGetLastError());
   return APHID_OK;
 }

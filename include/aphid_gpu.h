@@ -66,6 +66,8 @@ typedef struct {
   void *stream;      /* cudaStream_t to run on; NULL = a stream owned by the context */
   int graph_iters;   /* QMR iterations per CUDA-graph launch; 0 = default (16) */
   int verbose;       /* 1 = progress lines on stderr */
+  int plane_kz;      /* z-planes per block of the complex64 operator pass;
+                        0 = chosen from the mesh (the autotuner sets it) */
 } aphid_opts;
 
 typedef struct {
