@@ -68,8 +68,9 @@ struct aphid_ctx {
   int sw_nsys = 0;           // systems the buffers hold
   bool sw_f32_ok = false;    // complex64 vectors allocated
   double2 *sw_f64 = nullptr; // [2][nsys][n]: x64, b
-  float2 *sw_f32 = nullptr;  // [6][nsys][4][N]: v p q d x s (node layout)
-  ApplyMaps maps{};          // TMA tensor maps of the operator pass
+  float2 *sw_f32 = nullptr;  // [9][nsys][4][N]: 2 sets of q^ v^ p^, then d^ x^ D^-1 (node layout)
+  float4 *sw_ax32 = nullptr; // FP32 axis tables of the complex64 pass
+  PassMaps maps{};           // TMA tensor maps of the pass
   int *sw_err = nullptr;     // set by a kernel whose bounded wait gave up
   SweepSys *sw_sys = nullptr;
   double *sw_part = nullptr;
@@ -137,6 +138,8 @@ void release_work(aphid_ctx *ctx) {
   ctx->sw_gexec = nullptr;
   cudaFree(ctx->sw_f64);
   cudaFree(ctx->sw_f32);
+  cudaFree(ctx->sw_ax32);
+  ctx->sw_ax32 = nullptr;
   cudaFree(ctx->sw_sys);
   cudaFree(ctx->sw_part);
   cudaFree(ctx->sw_cnt);
@@ -697,22 +700,17 @@ int encode_map(aphid_ctx *ctx, CUtensorMap *m, CUtensorMapDataType type, int ran
   return APHID_OK;
 }
 
-// v~, p~, D^-1/2: 5-D (i, j, k, component, system) over 8-byte elements, one
-// box = 20 x 18 nodes of one z-plane, all four components
+// q^, v^, p^ of both buffer sets: 5-D (i, j, k, vector x component,
+// set x system) over 8-byte elements; one box = 20 x 18 nodes of one z-plane,
+// all three vectors and four components
 int vector_maps(aphid_ctx *ctx) {
   const NodeLayout &L = ctx->nl;
-  const size_t v32 = (size_t)ctx->sw_nsys * 4 * L.N;
-  const cuuint64_t dims[5] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4,
-                              (cuuint64_t)ctx->sw_nsys};
+  const cuuint64_t dims[5] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 12,
+                              2 * (cuuint64_t)ctx->sw_nsys};
   const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * 8, (cuuint64_t)L.nxp * ctx->ny * 8, (cuuint64_t)L.N * 8,
-                                 (cuuint64_t)L.N * 32};
-  const cuuint32_t box[5] = {kPW, kPH, 1, 4, 1};
-  int rc;
-  if ((rc = encode_map(ctx, &ctx->maps.v, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32, dims, strides, box)))
-    return rc;
-  if ((rc = encode_map(ctx, &ctx->maps.p, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + v32, dims, strides, box)))
-    return rc;
-  return encode_map(ctx, &ctx->maps.s, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + 5 * v32, dims, strides, box);
+                                 (cuuint64_t)L.N * 96};
+  const cuuint32_t box[5] = {kPW, kPH, 1, 12, 1};
+  return encode_map(ctx, &ctx->maps.w, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32, dims, strides, box);
 }
 
 // sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18
@@ -744,15 +742,15 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   D.epsr32 = ctx->d_epsr32;
   D.L = ctx->nl;
   D.err = ctx->sw_err;
+  D.tmix = 1.f;
   const size_t vec = (size_t)ctx->sw_nsys * ctx->n;
   const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
   if (ctx->sw_f32_ok) {
-    D.v = ctx->sw_f32;
-    D.p = ctx->sw_f32 + v32;
-    D.q = ctx->sw_f32 + 2 * v32;
-    D.d = ctx->sw_f32 + 3 * v32;
-    D.x = ctx->sw_f32 + 4 * v32;
-    D.s = ctx->sw_f32 + 5 * v32;
+    D.W = ctx->sw_f32;
+    D.dd = ctx->sw_f32 + 6 * v32;
+    D.xx = ctx->sw_f32 + 7 * v32;
+    D.dinv = ctx->sw_f32 + 8 * v32;
+    D.ax32 = ctx->sw_ax32;
   }
   D.x64 = ctx->sw_f64;
   D.b = ctx->sw_f64 + vec;
@@ -787,19 +785,19 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     }
     ctx->sw_bps = (int)std::max<long long>(
         1, std::min<long long>((ctx->n + kStreamThreads - 1) / kStreamThreads, std::max(4, 148 * 8 / nsys)));
-    // plane tiles: about 4 waves of 148 SMs x 3 blocks over the whole batch
+    // plane tiles: about 2 waves of 148 SMs x 2 blocks over the whole batch
     Tiles tp;
     tp.ti = (ctx->nx + kPTI - 1) / kPTI;
     tp.tj = (ctx->ny + kPTJ - 1) / kPTJ;
     const long long cols = (long long)tp.ti * tp.tj * nsys;
     tp.kz = ctx->plane_kz > 0
                 ? ctx->plane_kz
-                : (int)std::min<long long>(32, std::max<long long>(8, cols * ctx->nz / (148 * 3 * 2)));
+                : (int)std::min<long long>(32, std::max<long long>(4, cols * ctx->nz / (148 * 2 * 2)));
     tp.tk = (ctx->nz + tp.kz - 1) / tp.kz;
     ctx->ptiles = tp;
     ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()), tp.count());
     CK(cudaMalloc(&ctx->sw_sys, (size_t)nsys * sizeof(SweepSys)));
-    CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * 6 * sizeof(double)));
+    CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * kParts * sizeof(double)));
     CK(cudaMalloc(&ctx->sw_cnt, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
     CK(cudaMemset(ctx->sw_cnt, 0, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
     if (!ctx->sw_ndone) CK(cudaMalloc(&ctx->sw_ndone, sizeof(int)));
@@ -807,13 +805,19 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
   }
   if (mixed && !ctx->sw_f32_ok) {
     const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
-    if (cudaMalloc(&ctx->sw_f32, 6 * v32 * sizeof(float2)) != cudaSuccess) {
+    if (cudaMalloc(&ctx->sw_f32, 9 * v32 * sizeof(float2)) != cudaSuccess) {
       cudaGetLastError();
       ctx->sw_f32 = nullptr;
       return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex64 vectors failed");
     }
     // pads and components that do not exist stay zero for good
-    CK(cudaMemset(ctx->sw_f32, 0, 6 * v32 * sizeof(float2)));
+    CK(cudaMemset(ctx->sw_f32, 0, 9 * v32 * sizeof(float2)));
+    if (!ctx->sw_ax32) {
+      CK(cudaMalloc(&ctx->sw_ax32, 2 * (size_t)(ctx->nx + ctx->ny + ctx->nz) * sizeof(float4)));
+      const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));
+      k_sw_axis32<<<dim3((unsigned)((nmax + 127) / 128), 3), 128, 0, ctx->stream>>>(ctx->g, ctx->sw_ax32);
+      CK(cudaGetLastError());
+    }
     if (!ctx->sw_err) CK(cudaMalloc(&ctx->sw_err, sizeof(int)));
     ctx->sw_f32_ok = true;
     int rc = vector_maps(ctx);
@@ -863,32 +867,46 @@ static __global__ void k_sw_scatter(long long cnt, const long long *__restrict__
   if (t < cnt) b[idx[t]] = make_double2(val[t], 0.0);
 }
 
-size_t apply_shm(const SweepDev &D) { return kApplyShm + (D.epsr32 ? kApplyShmEps : 0); }
+size_t pass_shm(const SweepDev &D) { return D.epsr32 ? PassShm<true>::bytes : PassShm<false>::bytes; }
 
-// opt in to the dynamic shared memory of the operator pass (once per context)
-int apply_attrs(aphid_ctx *ctx) {
-  const int bytes = (int)(kApplyShm + kApplyShmEps);
-  CK(cudaFuncSetAttribute(k_sw_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  CK(cudaFuncSetAttribute(k_sw_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+// opt in to the dynamic shared memory of the pass (once per context)
+int pass_attrs(aphid_ctx *ctx) {
+  const int r = (int)PassShm<false>::bytes, e = (int)PassShm<true>::bytes;
+  CK(cudaFuncSetAttribute(k_sw_pass<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, r));
+  CK(cudaFuncSetAttribute(k_sw_pass<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, r));
+  CK(cudaFuncSetAttribute(k_sw_pass<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
+  CK(cudaFuncSetAttribute(k_sw_pass<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
   return APHID_OK;
+}
+
+void launch_pass(aphid_ctx *ctx, const SweepDev &D, bool timing) {
+  const unsigned sp = (unsigned)(D.tp.count() * D.nsys);
+  const size_t shm = pass_shm(D);
+  if (D.epsr32) {
+    if (timing)
+      k_sw_pass<true, true><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+    else
+      k_sw_pass<true, false><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+  } else {
+    if (timing)
+      k_sw_pass<false, true><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+    else
+      k_sw_pass<false, false><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+  }
 }
 
 void sweep_round(aphid_ctx *ctx, const SweepDev &D) {
   const unsigned ps = (unsigned)(D.bps * D.nsys);
   const unsigned st = (unsigned)(D.t.count() * D.nsys);
-  const unsigned sp = (unsigned)(D.tp.count() * D.nsys);
   k_sw_xupd<<<ps, kStreamThreads, 0, ctx->stream>>>(D);
   k_sw_resid<<<st, kOpThreads, 0, ctx->stream>>>(D);
-  for (int it = 0; it < ctx->graph_iters; it++) {
-    k_sw_apply<true><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D, ctx->maps);
-    k_sw_update<<<ps, kStreamThreads, 0, ctx->stream>>>(D);
-  }
+  for (int it = 0; it < ctx->graph_iters; it++) launch_pass(ctx, D, false);
   k_sw_check<<<st, kOpThreads, 0, ctx->stream>>>(D);
 }
 
 int sweep_graph(aphid_ctx *ctx, const SweepDev &D) {
   if (ctx->sw_gexec && ctx->sw_gkey == D.nsys) return APHID_OK;
-  int rc = apply_attrs(ctx);
+  int rc = pass_attrs(ctx);
   if (rc) return rc;
   if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
   ctx->sw_gexec = nullptr;
@@ -1041,11 +1059,11 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
   if (mixed) {
     k_sw_bnorm<<<(unsigned)(D.bps * nsys), kStreamThreads, 0, ctx->stream>>>(D);
     const dim3 sg((unsigned)((ctx->nx + 127) / 128), (unsigned)ctx->ny, (unsigned)(ctx->nz * nsys));
-    k_sw_scale<<<sg, 128, 0, ctx->stream>>>(D);
+    k_sw_dinv<<<sg, 128, 0, ctx->stream>>>(D);
     CK(cudaGetLastError());
     nlaunch += 2;
     if ((rc = sweep_graph(ctx, D))) return rc;
-    const long long per_round = 3 + 2LL * ctx->graph_iters;
+    const long long per_round = 3 + (long long)ctx->graph_iters;
     const long long max_rounds = (long long)std::max(1, opts->max_it) / ctx->graph_iters + 2LL * (hs[0].max_outer + 2);
     for (long long round = 0;; round++) {
       CK(cudaMemcpyAsync(ctx->h_ndone, ctx->sw_ndone, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1118,10 +1136,10 @@ int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {
   if (rc) return rc;
   if (ctx->sw_last < 1 || !ctx->sw_f32_ok || reps < 1)
     return fail(ctx, APHID_ERR_STATE, "no complex64 sweep state on the device");
-  const SweepDev D = sweep_dev(ctx, ctx->sw_last);
-  const unsigned sp = (unsigned)(D.tp.count() * D.nsys);
-  if ((rc = apply_attrs(ctx))) return rc;
-  for (int r = 0; r < reps; r++) k_sw_apply<false><<<sp, kPThreads, apply_shm(D), ctx->stream>>>(D, ctx->maps);
+  SweepDev D = sweep_dev(ctx, ctx->sw_last);
+  D.tmix = 0.f;
+  if ((rc = pass_attrs(ctx))) return rc;
+  for (int r = 0; r < reps; r++) launch_pass(ctx, D, true);
   CK(cudaGetLastError());
   return APHID_OK;
 }

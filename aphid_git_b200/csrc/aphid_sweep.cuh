@@ -6,30 +6,43 @@
 //   solve K e = r      complex64 QMR on the symmetrically Jacobi-scaled
 //                      operator K~ = D^-1/2 K D^-1/2 (D = gen_diag), FP64
 //                      inner products and Lanczos scalars
-//   x += D^-1/2 e~     FP64 accumulation
-// until ||r|| < target ||b||.  The Jacobi diagonal is FP64; its inverse square
-// root is stored once per system in complex64.  k^2 is never stored: it is
-// formed per system from the FP64 cell averages sigma-bar (and eps-bar) shared
-// by all systems, k^2 = i omega mu0 (sigma-bar + i omega eps0 eps-bar), which
-// is gen_k2_*grid (src/aphid.f90:1289-1535) for the linear models R, C, I.
+//   x += e             FP64 accumulation
+// until ||r|| < target ||b||.  The Jacobi diagonal is FP64; its inverse is
+// stored once per system in complex64.  k^2 is never stored: it is formed per
+// system from the cell averages sigma-bar (and eps-bar) shared by all
+// systems, k^2 = i omega mu0 (sigma-bar + i omega eps0 eps-bar), which is
+// gen_k2_*grid (src/aphid.f90:1289-1535) for the linear models R, C, I.
 //
 // Layout: x and b stay complex128 in the reference's [Ax|Ay|Az|Phi] order.
-// The complex64 inner state (v~, p~, q~, d~, x~, D^-1/2) is node-indexed:
-// [system][component][k][j][i] with rows padded to a multiple of 4 nodes, so
-// all four components of a node share one index, every row starts on a
-// 16-byte boundary (TMA-loadable), and components that do not exist at a
-// node (x at i = nx-1, ...) are stored zeros.
+// The complex64 inner state is node-indexed, [component][k][j][i] per vector
+// with rows padded to a multiple of 4 nodes, so all four components of a node
+// share one index, every row starts on a 16-byte boundary (TMA-loadable), and
+// components that do not exist at a node (x at i = nx-1, ...) are stored
+// zeros.
 //
-// The inner solver is the reference's coupled two-term QMR recurrence
-// (src/aphid_qmr.f90:297-372) with M = I on K~, two kernels per iteration:
-//   A  q~_n = K~ p~_n with p~_n = v~_n - k1 p~_{n-1} formed on the fly,
-//      epsilon_n = p~_n^T q~_n (= u^T K u with u = D^-1/2 p~_n);
-//   B  p~_n stored; vt = q~_n - beta_n v~_n stored unnormalised (v~_{n+1} =
-//      vt / rho_{n+1} is applied lazily through a scale factor), ||vt||^2
-//      and vt^T vt reduced; d~ and x~ updated one iteration late, because
-//      eta_n needs rho_{n+1} from this very reduction.
-// It keeps no residual vectors (r, s): the stop test uses the quasi-residual
-// norm tau_n = ||r~_0|| prod sqrt(theta_i c_i), an estimate that a
+// Inner solver: the reference's coupled two-term QMR recurrence
+// (src/aphid_qmr.f90:297-372) with M = I on K~, carried in "u-space": every
+// Krylov vector z~ of the scaled problem is stored as z^ = D^-1/2 z~, so the
+// operator is q^ = D^-1 K p^ (no scaling of the stencil's inputs), the
+// solution correction is x^ itself, and the scaled-space inner products are
+// weighted sums, z~^T y~ = sum D z^ y^ and ||z~||^2 = sum |D| |z^|^2.
+//
+// One fused pass per QMR iteration n (k_sw_pass).  It reads q^_{n-1},
+// v^_{n-1}, p^_{n-1} with halos and forms, per node,
+//   vt_n = q^_{n-1} - beta_{n-1} v^_{n-1},  v^_n = vt_n / rho_n,
+//   p^_n = v^_n - k1_n p^_{n-1}   (k1_n = rho_n delta_n / epsilon_{n-1}),
+// applies the stencil, q^_n = D^-1 K p^_n, applies the lagged update
+// d^_{n-1} = eta_{n-1} p^_{n-1} + kappa_{n-1} d^_{n-2}, x^ += d^_{n-1}, and
+// stores v^_n, p^_n, q^_n into the other buffer set (the halo reads of the
+// next pass must not see this pass's writes).  It reduces epsilon_n =
+// p~_n^T q~_n and the six inner products of v~_n and q~_n from which
+// rho_{n+1} = ||q~_n - beta_n v~_n|| and delta_{n+1} = v~_{n+1}^T v~_{n+1}
+// follow without another pass over the vectors (beta_n is not known until
+// the pass has finished).  The last block to finish runs the scalar
+// recurrences.  The expansions are accumulated in FP64 from per-node FP32
+// products; the cycle restarts from the FP64 residual when they lose accuracy
+// (see kCancel and kDrift).  No residual vectors are kept: the stop test uses
+// the quasi-residual tau_n = ||r~_0|| prod sqrt(theta_i c_i), which a
 // complex128 true-residual monitor checks once per graph round.
 //
 // Every system has a phase (OUTER -> INNER -> OUTER ... -> DONE);
@@ -43,30 +56,40 @@
 namespace aphid {
 
 enum { PH_OUTER = 0, PH_INNER = 2, PH_DONE = 3 };
-enum { CNT_RESID = 0, CNT_APPLY = 2, CNT_UPDATE = 3, CNT_BNORM = 4, CNT_CHECK = 5, CNT_KINDS = 6 };
+enum { CNT_RESID = 0, CNT_PASS = 2, CNT_BNORM = 4, CNT_CHECK = 5, CNT_KINDS = 6 };
+constexpr int kParts = 12;  // partial sums per slot and system
 
 // An inner cycle ends when the true residual, checked once per graph round,
 // falls this far behind its best tracking of the quasi-residual: the complex64
 // recurrence has reached its floor and only a restart from the FP64 residual
 // makes progress.
 constexpr double kStagnation = 16.0;
+// rho_{n+1}^2 from the expansion ||q||^2 - 2 Re(conj(beta) v^H q) + |beta|^2
+// ||v||^2 is trusted down to this fraction of ||q||^2; below it the new
+// Lanczos vector is treated as zero (the iterate is final for this cycle).
+constexpr double kCancel = 1e-10;
+// the cycle also restarts when the stored v~_n has drifted from ||v~_n|| = 1
+// or from v~_n^T v~_n = delta_n by more than this (relative)
+constexpr double kDrift = 1e-3;
 
 struct SweepSys {
   double omega, ka, kb;  // k^2 = (-ka * eps-bar, kb * sigma-bar)
   double rho_n, rho_np, c_n, c_nm, theta_n, theta_nm, kap, tau, tau0;
   double2 eps, del, beta, eta, k1;
-  double vscale;             // v~_n = vscale * (stored vt)
+  double vscale;             // 1 / rho_n
   double2 eta_pend;          // pending lagged update d = eta p + kap d
   double kap_pend;
   double bnorm, rnorm, inner_tol, target, rt0;
   double ratio_min, mon_rn;  // true-residual monitor of the running inner cycle
   int phase, has_inner, inner_it, total_it, outer_it, max_it, max_outer, status;
   int checks, pending;
+  int cur;                   // buffer set holding q^, v^, p^ of the last pass
+  int restarts;              // inner cycles ended by kCancel / kDrift
 };
 
-// plane tile of the complex64 operator pass: 16 x 16 nodes marching along k;
-// staged planes cover i0-2 .. i0+17 (20, even start: 16-byte TMA x origin)
-// and j0-1 .. j0+16 (18); sigma-bar planes cover i0-4 .. i0+19 (24).
+// plane tile of the complex64 pass: 16 x 16 nodes marching along k; staged
+// planes cover i0-2 .. i0+17 (20, even start: 16-byte TMA x origin) and
+// j0-1 .. j0+16 (18); sigma-bar planes cover i0-4 .. i0+19 (24).
 constexpr int kPTI = 16, kPTJ = 16, kPThreads = kPTI * kPTJ;
 constexpr int kPW = kPTI + 4, kPH = kPTJ + 2, kPN = kPW * kPH;   // 20 x 18
 constexpr int kKW = kPTI + 8, kKN = kKW * kPH;                    // 24 x 18
@@ -80,22 +103,28 @@ struct SweepDev {
   GridDev g;
   NodeLayout L;
   Tiles t;   // 32 x 4 column tiles (complex128 residual passes)
-  Tiles tp;  // 16 x 16 plane tiles (complex64 operator pass)
+  Tiles tp;  // 16 x 16 plane tiles (complex64 pass)
   long long n;           // unknowns per system (reference layout)
   int nsys, bps;         // systems; blocks per system of the pointwise kernels
   long long slots;       // partial-sum slots per system
   const double *sig;     // sigma-bar per unknown (FP64, reference layout)
   const double *epsr;    // eps-bar per unknown, or null (= 1)
-  const float *sig32, *epsr32;    // the same, FP32, node layout [4][N]
-  float2 *v, *p, *q, *d, *x, *s;  // [nsys][4][N] complex64, node layout (v holds vt)
-  double2 *x64, *b;               // [nsys][n] complex128, reference layout
+  const float *sig32, *epsr32;  // the same, FP32, node layout [4][N]
+  const float4 *ax32;    // per axis: [n] (n4, n5, dc, 1/dc), then [n] (e2, e3, d, 1/d) of edge m
+  float2 *W;             // [2 sets][nsys][q^, v^, p^][4][N] complex64
+  float2 *dd, *xx, *dinv;        // [nsys][4][N]: d^, x^, D^-1
+  double2 *x64, *b;              // [nsys][n] complex128, reference layout
   SweepSys *sys;
-  double *part;                   // [nsys][slots][6]
-  unsigned *cnt;                  // [CNT_KINDS][nsys]
+  double *part;                  // [nsys][slots][kParts]
+  unsigned *cnt;                 // [CNT_KINDS][nsys]
   int *ndone;
-  int *err;                       // set when a bounded wait gives up
+  int *err;                      // set when a bounded wait gives up
+  float tmix;                    // 1; 0 in timing launches (d^, x^ rewritten unchanged)
 };
 
+__device__ __forceinline__ float2 *wvec(const SweepDev &D, int set, int sys, int vec) {
+  return D.W + ((long long)(set * D.nsys + sys) * 3 + vec) * 4 * D.L.N;
+}
 __device__ __forceinline__ long long nd_of(const SweepDev &D, int i, int j, int k) {
   return i + (long long)D.L.nxp * (j + (long long)D.g.ny * k);
 }
@@ -206,32 +235,18 @@ struct K2Ref64 {  // k^2 from the FP64 averages (reference layout)
     return make_double2(-ka * e, kb * __ldg(sig + t));
   }
 };
-struct XRef64 {  // x (reference layout), optionally + D^-1/2 x~ (node layout)
+struct XRef64 {  // x (reference layout), optionally + x^ (node layout)
   GridDev g;
   const double2 *__restrict__ x64;
-  const float2 *__restrict__ s, *__restrict__ xt;  // null: x only
+  const float2 *__restrict__ xt;  // null: x only
   int nxp;
   long long N;
   __device__ __forceinline__ double2 operator()(int c, int i, int j, int k) const {
     double2 r = __ldg(x64 + ref_of(g, c, i, j, k));
-    if (xt) {
-      const long long t = c * N + i + (long long)nxp * (j + (long long)g.ny * k);
-      r = cadd(r, cmul(to_d(__ldg(s + t)), to_d(__ldg(xt + t))));
-    }
+    if (xt) r = cadd(r, to_d(__ldg(xt + c * N + i + (long long)nxp * (j + (long long)g.ny * k))));
     return r;
   }
 };
-
-// p~_n = vscale * vt - k1 p~_{n-1}, uncontracted so that the operator pass and
-// the update pass compute the same value
-__device__ __forceinline__ float2 vn32(float2 vt, float sc) {
-  return make_float2(__fmul_rn(sc, vt.x), __fmul_rn(sc, vt.y));
-}
-__device__ __forceinline__ float2 pnew32(float2 v, float2 p, float2 k1) {
-  const float re = __fsub_rn(__fmul_rn(k1.x, p.x), __fmul_rn(k1.y, p.y));
-  const float im = __fadd_rn(__fmul_rn(k1.x, p.y), __fmul_rn(k1.y, p.x));
-  return make_float2(__fsub_rn(v.x, re), __fsub_rn(v.y, im));
-}
 
 __device__ __forceinline__ void sweep_tile(const SweepDev &D, long long tile, int &i, int &j, int &k0,
                                            int &k1) {
@@ -252,7 +267,6 @@ __device__ __forceinline__ void mark_done(const SweepDev &D, SweepSys *S, int st
   atomicAdd(D.ndone, 1);
 }
 
-// ---------------------------------------------------------------- setup
 // sigma-bar / eps-bar per unknown: the area- and volume-weighted cell
 // averages of gen_k2_*grid before the factor i omega mu0, boundary values
 // from the clamped interior index (src/aphid.f90:1289-1535).
@@ -331,7 +345,7 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_bnorm(SweepDev D) 
   for (long long t = chunk * (long long)blockDim.x + threadIdx.x; t < D.n; t += (long long)D.bps * blockDim.x)
     a.v[0] += cabs2(b[t]);
   Vals<1> blk = block_reduce<1, kStreamThreads>(a);
-  double *part = D.part + (size_t)sys * D.slots * 6;
+  double *part = D.part + (size_t)sys * D.slots * kParts;
   if (arrive<1, kStreamThreads>(blk, part, D.cnt + CNT_BNORM * D.nsys + sys, chunk, D.bps)) {
     Vals<1> tot = final_reduce<1, kStreamThreads>(part, D.cnt + CNT_BNORM * D.nsys + sys, D.bps);
     if (threadIdx.x == 0) {
@@ -354,23 +368,26 @@ static __global__ void k_sw_to_node32(GridDev g, NodeLayout L, const double *__r
     node[c * L.N + nd] = exists(g, c, i, j, k) ? (float)ref[ref_of(g, c, i, j, k)] : 0.f;
 }
 
-// principal complex square root, then its reciprocal
-__device__ __forceinline__ double2 cinvsqrt(double2 z) {
-  const double m = hypot(z.x, z.y);
-  double2 r;
-  if (z.x >= 0.0) {
-    const double t = sqrt(0.5 * (m + z.x));
-    r = make_double2(t, t > 0 ? z.y / (2.0 * t) : 0.0);
-  } else {
-    const double t = sqrt(0.5 * (m - z.x));
-    r = make_double2(fabs(z.y) / (2.0 * t), copysign(t, z.y));
-  }
-  return cdiv(make_double2(1.0, 0.0), r);
+
+// FP32 axis tables of the complex64 pass, built once per mesh:
+// [m] = (n4, n5, dc, 1/dc) of node m and [n + m] = (e2, e3, d, 1/d) of the
+// edge (m, m+1) (zeros and ones past the last edge).
+static __global__ void k_sw_axis32(GridDev g, float4 *out) {
+  const int a = blockIdx.y;
+  const Axis A = a == 0 ? g.ax[0] : (a == 1 ? g.ax[1] : g.ax[2]);
+  const int n = A.n, m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const int base = a == 0 ? 0 : (a == 1 ? 2 * g.ax[0].n : 2 * (g.ax[0].n + g.ax[1].n));
+  out[base + m] = make_float4((float)A.n4[m], (float)A.n5[m], (float)A.dc[m], (float)(1.0 / A.dc[m]));
+  const bool e = m < n - 1;
+  out[base + n + m] = make_float4(e ? (float)A.e2[m] : 0.f, e ? (float)A.e3[m] : 0.f, e ? (float)A.d[m + 1] : 1.f,
+                                  e ? (float)(1.0 / A.d[m + 1]) : 1.f);
 }
 
-// D^-1/2 per node, component and system from the FP64 Jacobi diagonal
-// (gen_diag, src/aphid.f90:1542-1725, with k^2 from the averages)
-static __global__ void k_sw_scale(SweepDev D) {
+// D^-1 per node, component and system from the FP64 Jacobi diagonal
+// (gen_diag, src/aphid.f90:1542-1725, with k^2 from the averages); zero where
+// a component does not exist, 1 on boundary nodes (diag_p = 1).
+static __global__ void k_sw_dinv(SweepDev D) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z % D.g.nz;
   const int sys = blockIdx.z / D.g.nz;
   const GridDev &g = D.g;
@@ -386,23 +403,24 @@ static __global__ void k_sw_scale(SweepDev D) {
   const double xn4 = mask_hi(I, nx) / dxi / dxci, xn5 = mask_lo(I, nx) / dxim / dxci;
   const double yn4 = mask_hi(J, ny) / dyj / dycj, yn5 = mask_lo(J, ny) / dyjm / dycj;
   const double zn4 = mask_hi(KK, nz) / dzk / dzck, zn5 = mask_lo(KK, nz) / dzkm / dzck;
-  float2 *s = D.s + (long long)sys * 4 * D.L.N;
+  const double2 one = make_double2(1.0, 0.0);
+  float2 *dv = D.dinv + (long long)sys * 4 * D.L.N;
   const long long nd = nd_of(D, i, j, k);
   float2 o[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(1.f, 0.f)};
   if (i < nx - 1) {
     const double c2 = mask_hi(I, nx - 1) / (0.5 * (dxi + dx[I + 1])) / dxi, c3 = mask_lo(I, nx) / dxci / dxi;
     const double2 kv = K(0, i, j, k);
-    o[0] = to_f(cinvsqrt(rmul(dxi * dycj * dzck, make_double2(-(c2 + c3 + yn4 + yn5 + zn4 + zn5) + kv.x, kv.y))));
+    o[0] = to_f(cdiv(one, rmul(dxi * dycj * dzck, make_double2(-(c2 + c3 + yn4 + yn5 + zn4 + zn5) + kv.x, kv.y))));
   }
   if (j < ny - 1) {
     const double c2 = mask_hi(J, ny - 1) / (0.5 * (dyj + dy[J + 1])) / dyj, c3 = mask_lo(J, ny) / dycj / dyj;
     const double2 kv = K(1, i, j, k);
-    o[1] = to_f(cinvsqrt(rmul(dxci * dyj * dzck, make_double2(-(c2 + c3 + xn4 + xn5 + zn4 + zn5) + kv.x, kv.y))));
+    o[1] = to_f(cdiv(one, rmul(dxci * dyj * dzck, make_double2(-(c2 + c3 + xn4 + xn5 + zn4 + zn5) + kv.x, kv.y))));
   }
   if (k < nz - 1) {
     const double c2 = mask_hi(KK, nz - 1) / (0.5 * (dzk + dz[KK + 1])) / dzk, c3 = mask_lo(KK, nz) / dzck / dzk;
     const double2 kv = K(2, i, j, k);
-    o[2] = to_f(cinvsqrt(rmul(dxci * dycj * dzk, make_double2(-(c2 + c3 + xn4 + xn5 + yn4 + yn5) + kv.x, kv.y))));
+    o[2] = to_f(cdiv(one, rmul(dxci * dycj * dzk, make_double2(-(c2 + c3 + xn4 + xn5 + yn4 + yn5) + kv.x, kv.y))));
   }
   if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1) {
     const double2 s1 = K(3, i, j, k);
@@ -413,15 +431,15 @@ static __global__ void k_sw_scale(SweepDev D) {
     const double2 c6 = rdiv(rdiv(rmul(mask_hi(KK, nz), K(2, i, j, k)), dzk), dzck);
     const double2 c7 = rdiv(rdiv(rmul(mask_lo(KK, nz), K(2, i, j, k - 1)), dzkm), dzck);
     const double2 sum = cadd(cadd(cadd(cadd(cadd(c2, c3), c4), c5), c6), c7);
-    o[3] = to_f(cinvsqrt(rmul(dxci * dycj * dzck, cadd(cneg(sum), cmul(s1, s1)))));
+    o[3] = to_f(cdiv(one, rmul(dxci * dycj * dzck, cadd(cneg(sum), cmul(s1, s1)))));
   }
 #pragma unroll
-  for (int c = 0; c < 4; c++) s[c * D.L.N + nd] = o[c];
+  for (int c = 0; c < 4; c++) dv[c * D.L.N + nd] = o[c];
 }
 
 // ------------------------------------------------------------ outer step
-// O1: x += D^-1/2 (x~ + pending lagged update), FP64 accumulation of the
-// inner correction into the reference-layout solution
+// O1: x += x^ (+ the pending lagged update), FP64 accumulation of the inner
+// correction into the reference-layout solution
 static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
   const int sys = blockIdx.x % D.nsys, chunk = blockIdx.x / D.nsys;
   const SweepSys *S = D.sys + sys;
@@ -430,6 +448,7 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
   const bool pend = S->pending != 0;
   const double2 eta = S->eta_pend;
   const double kap = S->kap_pend;
+  const float2 *P = wvec(D, S->cur, sys, 2), *dd = D.dd + vb, *xx = D.xx + vb;
   const GridDev &g = D.g;
   const long long plane = (long long)D.L.nxp * g.ny;
   double2 *x64 = D.x64 + (long long)sys * D.n;
@@ -442,18 +461,18 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       if (!exists(g, c, i, j, k)) continue;
-      const long long t = vb + c * D.L.N + nd;
-      double2 xt = to_d(D.x[t]);
-      if (pend) xt = cadd(xt, cadd(cmul(eta, to_d(D.p[t])), rmul(kap, to_d(D.d[t]))));
+      const long long t = c * D.L.N + nd;
+      double2 xt = to_d(xx[t]);
+      if (pend) xt = cadd(xt, cadd(cmul(eta, to_d(P[t])), rmul(kap, to_d(dd[t]))));
       const long long rt = ref_of(g, c, i, j, k);
-      x64[rt] = cadd(x64[rt], cmul(to_d(D.s[t]), xt));
+      x64[rt] = cadd(x64[rt], xt);
     }
   }
 }
 
-// O2: r = b - K x in complex128 (true residual); r~ = D^-1/2 r starts the
-// next inner cycle: stored (complex64) as the unnormalised first Lanczos
-// vector, p~ = d~ = x~ = 0, and the inner scalars of
+// O2: r = b - K x in complex128 (true residual).  The next inner cycle starts
+// from r~_0 = D^-1/2 r, stored as q^ = D^-1 r with v^ = p^ = d^ = x^ = 0 and
+// beta_0 = 0, so that the first pass forms v~_1 = r~_0 / ||r~_0||; scalars of
 // src/aphid_qmr.f90:268-285, 299-313 with M = I.
 static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
   const int sys = blockIdx.x % D.nsys;
@@ -464,10 +483,11 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
   sweep_tile(D, tile, i, j, k0, k1);
   Vals<4> a{{0.0, 0.0, 0.0, 0.0}};
   if (i < D.g.nx && j < D.g.ny) {
-    const XRef64 L{D.g, D.x64 + (long long)sys * D.n, nullptr, nullptr, D.L.nxp, D.L.N};
+    const XRef64 L{D.g, D.x64 + (long long)sys * D.n, nullptr, D.L.nxp, D.L.N};
     const K2Ref64 K{D.g, D.sig, D.epsr, S->ka, S->kb};
     const double2 *b = D.b + (long long)sys * D.n;
     const long long vb = (long long)sys * 4 * D.L.N;
+    float2 *Q = wvec(D, S->cur, sys, 0), *V = wvec(D, S->cur, sys, 1), *P = wvec(D, S->cur, sys, 2);
     const float2 zero = make_float2(0.f, 0.f);
     for (int k = k0; k < k1; k++) {
       double2 o[4];
@@ -475,27 +495,32 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
       const long long nd = nd_of(D, i, j, k);
 #pragma unroll
       for (int c = 0; c < 4; c++) {
-        const long long t = vb + c * D.L.N + nd;
-        float2 rt = zero;
+        const long long t = c * D.L.N + nd;
+        float2 rq = zero;
         if (exists(D.g, c, i, j, k)) {
           const double2 r = csub(b[ref_of(D.g, c, i, j, k)], o[c]);
-          rt = to_f(cmul(to_d(D.s[t]), r));
-          const double2 drt = to_d(rt);
+          const double2 di = to_d(D.dinv[vb + t]);
+          rq = to_f(cmul(di, r));
           a.v[0] += cabs2(r);
-          a.v[1] += cabs2(drt);
-          const double2 sq = cmul(drt, drt);
-          a.v[2] += sq.x;
-          a.v[3] += sq.y;
+          const double m2 = cabs2(di);
+          if (m2 > 0.0) {
+            const double2 q = to_d(rq);
+            a.v[1] += cabs2(q) / sqrt(m2);        // ||r~||^2 = sum |D| |q^|^2
+            const double2 w = cdiv(cmul(q, q), di);  // r~^T r~ = sum D q^2
+            a.v[2] += w.x;
+            a.v[3] += w.y;
+          }
         }
-        D.v[t] = rt;
-        D.p[t] = zero;
-        D.d[t] = zero;
-        D.x[t] = zero;
+        Q[t] = rq;
+        V[t] = zero;
+        P[t] = zero;
+        D.dd[vb + t] = zero;
+        D.xx[vb + t] = zero;
       }
     }
   }
   Vals<4> blk = block_reduce<4, kOpThreads>(a);
-  double *part = D.part + (size_t)sys * D.slots * 6;
+  double *part = D.part + (size_t)sys * D.slots * kParts;
   unsigned *cnt = D.cnt + CNT_RESID * D.nsys + sys;
   const unsigned nt = (unsigned)D.t.count();
   if (arrive<4, kOpThreads>(blk, part, cnt, (unsigned)tile, nt)) {
@@ -519,6 +544,7 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
         S->eps = make_double2(1.0, 0.0);
         S->theta_n = 0.0;
         S->eta = make_double2(-1.0, 0.0);
+        S->beta = make_double2(0.0, 0.0);
         S->rho_np = rt0;
         S->c_nm = 1.0;
         S->rho_n = rt0;
@@ -538,10 +564,10 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
   }
 }
 
-// Monitor: the true residual of the running iterate, ||b - K (x + D^-1/2 x~)||
-// in complex128 (x~ lags one update), once per graph round.  Ends the inner
+// Monitor: the true residual of the running iterate, ||b - K (x + x^)|| in
+// complex128 (x^ lags one update), once per graph round.  Ends the inner
 // cycle on convergence or on stagnation of the complex64 recurrence (see
-// kStagnation); the next round's outer step folds x~ into x and restarts
+// kStagnation); the next round's outer step folds x^ into x and restarts
 // from the FP64 residual.
 static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
   const int sys = blockIdx.x % D.nsys;
@@ -553,7 +579,7 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
   Vals<1> a{{0.0}};
   if (i < D.g.nx && j < D.g.ny) {
     const long long vb = (long long)sys * 4 * D.L.N;
-    const XRef64 L{D.g, D.x64 + (long long)sys * D.n, D.s + vb, D.x + vb, D.L.nxp, D.L.N};
+    const XRef64 L{D.g, D.x64 + (long long)sys * D.n, D.xx + vb, D.L.nxp, D.L.N};
     const K2Ref64 K{D.g, D.sig, D.epsr, S->ka, S->kb};
     const double2 *b = D.b + (long long)sys * D.n;
     for (int k = k0; k < k1; k++) {
@@ -565,7 +591,7 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
     }
   }
   Vals<1> blk = block_reduce<1, kOpThreads>(a);
-  double *part = D.part + (size_t)sys * D.slots * 6;
+  double *part = D.part + (size_t)sys * D.slots * kParts;
   unsigned *cnt = D.cnt + CNT_CHECK * D.nsys + sys;
   const unsigned nt = (unsigned)D.t.count();
   if (arrive<1, kOpThreads>(blk, part, cnt, (unsigned)tile, nt)) {
@@ -623,48 +649,119 @@ __device__ __forceinline__ void tma_load4(unsigned dst, const CUtensorMap *map, 
 }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-// tensor maps of the operator pass (kernel parameter, __grid_constant__)
-struct ApplyMaps {
-  CUtensorMap s, v, p;  // 5-D: (nxp, ny, nz, component, system), 8-byte elements
-  CUtensorMap sig, eps; // 4-D: (nxp, ny, nz, component), FP32
+// tensor maps of the pass (kernel parameter, __grid_constant__)
+struct PassMaps {
+  CUtensorMap w;         // 5-D: (nxp, ny, nz, vector x component = 12, set x system), 8-byte elements
+  CUtensorMap sig, eps;  // 4-D: (nxp, ny, nz, component), FP32
 };
 
-constexpr unsigned kRawBytes = 4u * kPN * 8u;   // one array, four components, one plane
-constexpr unsigned kSigBytes = 4u * kKN * 4u;
-constexpr size_t kApplyShm = 3 * (size_t)kRawBytes   // raw s, v, p of one plane
-                           + 3 * (size_t)kRawBytes   // U ring (three planes)
-                           + 2 * (size_t)kSigBytes   // sigma-bar, two planes
-                           + 128;                    // mbarriers (keeps what follows 128-byte aligned)
-constexpr size_t kApplyShmEps = 2 * (size_t)kSigBytes;  // eps-bar, two planes (models C, I)
+constexpr unsigned kVecPlane = kPN * 8u;         // one component of one vector, one staged plane
+constexpr unsigned kRawBytes = 12u * kVecPlane;  // q^, v^, p^, four components each
+constexpr unsigned kSigBytes = 4u * kKN * 4u;    // sigma-bar, four components
+constexpr unsigned kUBytes = 4u * kVecPlane;     // u of one plane
+// shared memory of the pass: two load stages (q^ v^ p^ of plane m+1 and
+// sigma-bar [eps-bar] of plane m), two u planes, the mbarriers
+template <bool EPS>
+struct PassShm {
+  static constexpr unsigned stage = kRawBytes + (EPS ? 2u : 1u) * kSigBytes;
+  static constexpr size_t bytes = 2 * (size_t)stage + 2 * (size_t)kUBytes + 128;
+};
 constexpr int kWaitTries = 1 << 24;
 
-// A: q~_n = D^-1/2 K D^-1/2 p~_n and epsilon_n = u^T K u (u = D^-1/2 p~_n),
-// then beta_n = epsilon_n / delta_n (src/aphid_qmr.f90:324-330).
-//
-// A 16 x 16 node tile marches along k.  One thread issues, per z-plane, three
-// TMA loads (v~, p~, D^-1/2: all four components, 20 x 18 nodes with halo)
-// and one for sigma-bar; the loads of plane k+2 (and sigma-bar of k+1) are in
-// flight while plane k is computed.  u = D^-1/2 (vscale vt - k1 p~) is formed
-// once per point into a ring of three planes.  TMA fills outside the tensor
-// with zeros, pads and non-existent components are stored zeros, so zero
-// padding reproduces the reference's clamped neighbours (their coefficients
-// are zero at the boundary).
-// SCALARS = false: the same pass without the scalar step and the phase test
-// (operator timing on resident data; never changes a system's state).
-template <bool SCALARS>
-__global__ void __launch_bounds__(kPThreads, 2) k_sw_apply(SweepDev D, const __grid_constant__ ApplyMaps M) {
+__device__ __forceinline__ float2 axpy(float a, float2 x, float2 y) {
+  return make_float2(fmaf(a, x.x, y.x), fmaf(a, x.y, y.y));
+}
+__device__ __forceinline__ float2 cfma(float2 a, float2 x, float2 y) {  // y + a x
+  return make_float2(fmaf(a.x, x.x, fmaf(-a.y, x.y, y.x)), fmaf(a.x, x.y, fmaf(a.y, x.x, y.y)));
+}
+
+// Scalar step at the end of pass n (one thread): epsilon_n, beta_n,
+// rho_{n+1} and delta_{n+1} from the pipelined inner products, then theta,
+// c, eta, kappa, tau and k1 as in src/aphid_qmr.f90:324-372.
+__device__ __noinline__ void pass_scalars(SweepSys *S, const double *T) {
+  S->cur ^= 1;
+  S->inner_it++;
+  S->total_it++;
+  S->pending = 0;
+  const double2 e = make_double2(T[0], T[1]);
+  S->eps = e;
+  if (!finite2(e) || zero2(e)) {  // breakdown: restart from the current x
+    S->phase = PH_OUTER;
+    return;
+  }
+  const double2 beta = cdiv(e, S->del);
+  const double A1 = T[2], A3 = T[5];
+  const double2 A2 = make_double2(T[3], T[4]), B1 = make_double2(T[6], T[7]);
+  const double2 B2 = make_double2(T[8], T[9]), B3 = make_double2(T[10], T[11]);
+  const double bb = cabs2(beta);
+  double rho2 = A1 - 2.0 * (beta.x * A2.x + beta.y * A2.y) + bb * A3;
+  if (!isfinite(rho2) || !(bb > 0.0)) {
+    S->phase = PH_OUTER;
+    return;
+  }
+  const bool exhausted = !(rho2 > kCancel * A1);  // Krylov space exhausted (or below the expansion's accuracy)
+  if (exhausted) rho2 = 0.0;
+  const double rho = sqrt(rho2);
+  S->beta = beta;
+  S->rho_np = rho;
+  S->theta_n = rho2 / S->c_nm / bb;
+  S->c_n = 1.0 / (1.0 + S->theta_n);
+  S->eta = cdiv(rmul(S->c_n, rmul(S->rho_n, cneg(S->eta))), rmul(S->c_nm, beta));
+  S->kap = S->theta_nm * S->c_n;
+  S->tau = S->tau * sqrt(S->theta_n * S->c_n);
+  S->eta_pend = S->eta;
+  S->kap_pend = S->kap;
+  S->pending = finite2(S->eta) && isfinite(S->kap);
+  if (exhausted) {
+    S->phase = PH_OUTER;
+    return;
+  }
+  const double2 vtv = cadd(csub(B1, rmul(2.0, cmul(beta, B2))), cmul(cmul(beta, beta), B3));
+  const double2 del = rmul(1.0 / rho2, vtv);
+  const bool drift = fabs(A3 - 1.0) > kDrift || sqrt(cabs2(csub(B3, S->del))) > kDrift * sqrt(cabs2(S->del));
+  if (drift) S->restarts++;
+  if (!S->pending || !isfinite(S->tau) || !finite2(del) || zero2(del) || drift ||
+      S->tau < S->inner_tol * S->tau0 || S->total_it >= S->max_it) {
+    S->phase = PH_OUTER;
+    return;
+  }
+  S->c_nm = S->c_n;
+  S->rho_n = rho;
+  S->theta_nm = S->theta_n;
+  S->del = del;
+  S->k1 = cdiv(rmul(rho, del), e);
+  S->vscale = 1.0 / rho;
+}
+
+// The fused QMR pass (see the file comment).  A 16 x 16 node tile marches
+// along k.  Thread 0 issues, per z-plane, one TMA load of q^, v^, p^ (all
+// four components, 20 x 18 nodes with halo) and one of sigma-bar (eps-bar)
+// into a two-stage ring: the loads of step m+1 are in flight while plane m
+// is computed.  Each thread forms u = p^_n of its own node (which also gives
+// v^_n, the stored outputs and the lagged update) and one halo value, into
+// the u plane of the next step; the z-neighbours of its own node stay in
+// registers.  TMA fills outside the tensor with zeros, and pads and absent
+// components are stored zeros, so zero padding reproduces the reference's
+// clamped neighbours (their coefficients are zero at the boundary).
+// EPS: models C and I (eps-bar not 1).  TIMING: the same pass over resident
+// data without the phase test and the scalar step, leaving d^ and x^ as they
+// were; it flips the buffer set like an iteration does, so consecutive timing
+// launches read what the previous one wrote (the x64 solution is untouched).
+template <bool EPS, bool TIMING>
+__global__ void __launch_bounds__(kPThreads, EPS ? 1 : 2) k_sw_pass(SweepDev D, const __grid_constant__ PassMaps M) {
   const int sys = blockIdx.x % D.nsys;
   const long long tile = blockIdx.x / D.nsys;
   SweepSys *S = D.sys + sys;
-  if (SCALARS && S->phase != PH_INNER) return;
+  if (!TIMING && S->phase != PH_INNER) return;
+  constexpr unsigned kStage = PassShm<EPS>::stage;
   extern __shared__ __align__(128) unsigned char shm[];
-  float2 *RAW = reinterpret_cast<float2 *>(shm);                          // [3][4][kPN]: s, v, p
-  float2 *U = reinterpret_cast<float2 *>(shm + 3 * kRawBytes);            // [3][4][kPN]
-  float *RK = reinterpret_cast<float *>(shm + 6 * kRawBytes);             // [2][4][kKN]
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + 6 * kRawBytes + 2 * kSigBytes);
-  const bool has_eps = D.epsr32 != nullptr;
-  float *RE = reinterpret_cast<float *>(shm + kApplyShm);                 // [2][4][kKN]
-  const unsigned b_raw = smem_u32(&bar[0]), b_k0 = smem_u32(&bar[1]), b_k1 = smem_u32(&bar[2]);
+  float2 *Ub = reinterpret_cast<float2 *>(shm + 2 * kStage);  // [2][4][kPN]
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + 2 * kStage + 2 * kUBytes);
+  // TMA destinations must be 128-byte aligned: refuse to copy otherwise
+  if (smem_u32(shm) & 127u) {
+    if (threadIdx.x == 0) atomicExch(D.err, 2);
+    return;
+  }
 
   const GridDev &g = D.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -676,301 +773,362 @@ __global__ void __launch_bounds__(kPThreads, 2) k_sw_apply(SweepDev D, const __g
   const int i0 = bi * kPTI, j0 = bj * kPTJ, k0 = bk * D.tp.kz, k1 = min(nz, k0 + D.tp.kz);
   const int tx = threadIdx.x % kPTI, ty = threadIdx.x / kPTI;
   const int i = i0 + tx, j = j0 + ty;
-  const long long N = D.L.N;
-  const float2 *__restrict__ sv = D.s + (long long)sys * 4 * N;
-  float2 *__restrict__ q = D.q + (long long)sys * 4 * N;
+  const bool live = i < nx && j < ny;
+  const long long N = D.L.N, plane = (long long)D.L.nxp * ny;
+  const long long ndc = i + (long long)D.L.nxp * j;  // this node within a plane
+  const int cur = S->cur;
+  const long long sb = (long long)sys * 4 * N;
+  float2 *__restrict__ Qw = wvec(D, cur ^ 1, sys, 0);
+  float2 *__restrict__ Vw = wvec(D, cur ^ 1, sys, 1);
+  float2 *__restrict__ Pw = wvec(D, cur ^ 1, sys, 2);
+  float2 *__restrict__ dd = D.dd + sb;
+  float2 *__restrict__ xx = D.xx + sb;
+  const float2 *__restrict__ dv = D.dinv + sb;
   const float *__restrict__ sig = D.sig32;
   const float *__restrict__ eps = D.epsr32;
-  const float2 kone = to_f(S->k1);
-  const float vsc = (float)S->vscale;
-  const float ka = (float)S->ka, kb = (float)S->kb;
-  int *err = D.err;
-
-  // TMA destinations must be 128-byte aligned: refuse to copy otherwise
-  if (smem_u32(shm) & 127u) {
-    if (threadIdx.x == 0) atomicExch(D.err, 2);
-    return;
+  // u = ca q^ + cb v^ + cc p^ and v = ca q^ + cb v^
+  const float ca = (float)S->vscale;
+  const float2 cb = to_f(rmul(-S->vscale, S->beta));
+  const float2 cc = to_f(cneg(S->k1));
+  const bool pend = TIMING || S->pending != 0;
+  // timing launches rewrite d^ and x^ with their own values through the same
+  // arithmetic (eta = 0, kappa = 1, x^ += 0 d^), the zeros coming from a
+  // runtime value so that the loads and stores stay in the code
+  const float xmix = TIMING ? D.tmix : 1.f;
+  float2 eta = to_f(S->eta_pend);
+  float kap = (float)S->kap_pend;
+  if (TIMING) {
+    eta = xmix != 0.f ? eta : make_float2(0.f, 0.f);
+    kap = xmix != 0.f ? kap : 1.f;
   }
+  const float ka = (float)S->ka, kb = (float)S->kb;
+  const int wset = cur * D.nsys + sys;  // TMA coordinate of the read set
+
+  const unsigned b0 = smem_u32(&bar[0]), b1 = smem_u32(&bar[1]);
   if (threadIdx.x == 0) {
-    mbar_init(b_raw);
-    mbar_init(b_k0);
-    mbar_init(b_k1);
+    mbar_init(b0);
+    mbar_init(b1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     fence_async_smem();
   }
   __syncthreads();
-  unsigned ph_raw = 0, ph_k[2] = {0, 0};
+  unsigned ph0 = 0, ph1 = 0;
 
-  auto issue_raw = [&](int kk) {  // thread 0: v~, p~, D^-1/2 of plane kk
+  // thread 0: the loads of step m into stage st (q^ v^ p^ of plane m+1,
+  // sigma-bar and eps-bar of plane m)
+  auto issue = [&](int st, int m) {
+    const unsigned bb = st ? b1 : b0;
+    unsigned char *base = shm + st * kStage;
     fence_async_smem();
-    mbar_expect(b_raw, 3 * kRawBytes);
-    tma_load5(smem_u32(RAW), &M.s, i0 - 2, j0 - 1, kk, 0, sys, b_raw);
-    tma_load5(smem_u32(RAW + 4 * kPN), &M.v, i0 - 2, j0 - 1, kk, 0, sys, b_raw);
-    tma_load5(smem_u32(RAW + 8 * kPN), &M.p, i0 - 2, j0 - 1, kk, 0, sys, b_raw);
+    mbar_expect(bb, kStage);
+    tma_load5(smem_u32(base), &M.w, i0 - 2, j0 - 1, m + 1, 0, wset, bb);
+    tma_load4(smem_u32(base + kRawBytes), &M.sig, i0 - 4, j0 - 1, m, 0, bb);
+    if (EPS) tma_load4(smem_u32(base + kRawBytes + kSigBytes), &M.eps, i0 - 4, j0 - 1, m, 0, bb);
   };
-  auto issue_k = [&](int kk, int buf) {  // thread 0: sigma-bar (eps-bar) of plane kk
-    fence_async_smem();
-    const unsigned bb = buf ? b_k1 : b_k0;
-    mbar_expect(bb, has_eps ? 2 * kSigBytes : kSigBytes);
-    tma_load4(smem_u32(RK + buf * 4 * kKN), &M.sig, i0 - 4, j0 - 1, kk, 0, bb);
-    if (has_eps) tma_load4(smem_u32(RE + buf * 4 * kKN), &M.eps, i0 - 4, j0 - 1, kk, 0, bb);
+  auto wait = [&](int st) {
+    const bool ok = st ? mbar_wait(b1, ph1, kWaitTries) : mbar_wait(b0, ph0, kWaitTries);
+    if (!ok && threadIdx.x == 0) atomicExch(D.err, 1);
+    if (st)
+      ph1 ^= 1u;
+    else
+      ph0 ^= 1u;
   };
-  auto wait_raw = [&]() {
-    if (!mbar_wait(b_raw, ph_raw, kWaitTries) && threadIdx.x == 0) atomicExch(err, 1);
-    ph_raw ^= 1u;
-  };
-  auto wait_k = [&](int buf) {
-    if (!mbar_wait(buf ? b_k1 : b_k0, ph_k[buf], kWaitTries) && threadIdx.x == 0) atomicExch(err, 1);
-    ph_k[buf] ^= 1u;
-  };
-  auto convert = [&](int kk) {  // raw plane -> u = D^-1/2 (vscale vt - k1 p~) in the ring
-    float2 *Us = U + ((kk - k0 + 3) % 3) * 4 * kPN;
-    for (int e = threadIdx.x; e < 4 * kPN; e += kPThreads)
-      Us[e] = cmul(RAW[e], pnew32(vn32(RAW[4 * kPN + e], vsc), RAW[8 * kPN + e], kone));
+  auto combine = [&](float2 q, float2 v, float2 p, float2 &vo) {
+    vo = cfma(cb, v, make_float2(ca * q.x, ca * q.y));
+    return cfma(cc, p, vo);
   };
 
-  // prologue: planes k0-1, k0, k0+1 into the ring, sigma-bar of k0
-  for (int kk = k0 - 1; kk <= k0 + 1; kk++) {
-    if (threadIdx.x == 0) issue_raw(kk);
-    wait_raw();
-    convert(kk);
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) issue_k(k0, 0);
-
-  double ea = 0.0, eb = 0.0;
-  const bool live = i < nx && j < ny;
-  const int c0 = (ty + 1) * kPW + (tx + 2);  // this node in a staged plane
+  const int eo = (ty + 1) * kPW + (tx + 2);  // this node in a staged plane
   const int ck = (ty + 1) * kKW + (tx + 4);  // this node in a sigma-bar plane
-  const Axis &X = g.ax[0], &Y = g.ax[1], &Z = g.ax[2];
-  const float xn4 = live ? (float)X.n4[i] : 0.f, xn5 = live ? (float)X.n5[i] : 0.f;
-  const float yn4 = live ? (float)Y.n4[j] : 0.f, yn5 = live ? (float)Y.n5[j] : 0.f;
-  const float dxc = live ? (float)X.dc[i] : 1.f, dyc = live ? (float)Y.dc[j] : 1.f;
-  const bool hx = live && i < nx - 1, hy = live && j < ny - 1;
-  const float ce2x = hx ? (float)X.e2[i] : 0.f, ce3x = hx ? (float)X.e3[i] : 0.f;
-  const float dxi = hx ? (float)X.d[i + 1] : 1.f;
-  const float ce2y = hy ? (float)Y.e2[j] : 0.f, ce3y = hy ? (float)Y.e3[j] : 0.f;
-  const float dyj = hy ? (float)Y.d[j + 1] : 1.f;
-  const bool pin = live && i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
-  const long long plane = (long long)D.L.nxp * ny;
-  const long long ndc = i + (long long)D.L.nxp * j;  // node index within a plane
+  // the one halo value this thread forms per plane: component hc on side hs
+  const int hc = threadIdx.x >> 6, hh = threadIdx.x & 63, hs = hh >> 4, hr = hh & 15;
+  const int he = hs < 2 ? (hr + 1) * kPW + (hs == 0 ? 1 : kPTI + 2) : (hs == 2 ? 0 : (kPTJ + 1) * kPW) + hr + 2;
 
-  for (int k = k0; k < k1; k++) {
-    const int kb_ = (k - k0) & 1;
-    const bool more = k + 1 < k1;
-    if (more && threadIdx.x == 0) {
-      issue_raw(k + 2);
-      issue_k(k + 1, kb_ ^ 1);
+  float2 um[4], uc[4], up[4], vc[4], vn[4];
+  // own node of plane m1 from stage st: u (into the u plane and registers),
+  // v^_n; when the node is this block's: v^_n, p^_n stored and the lagged
+  // d^, x^ update
+  auto own_step = [&](int st, int m1, float2 *Us, float2 (&uo)[4], float2 (&vo)[4]) {
+    const float2 *R = reinterpret_cast<const float2 *>(shm + st * kStage);
+    const bool owned = live && m1 < k1;
+    const long long nd = ndc + m1 * plane;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const float2 p = R[(8 + c) * kPN + eo];
+      uo[c] = combine(R[c * kPN + eo], R[(4 + c) * kPN + eo], p, vo[c]);
+      Us[c * kPN + eo] = uo[c];
+      if (owned) {
+        const long long t = c * N + nd;
+        Vw[t] = vo[c];
+        Pw[t] = uo[c];
+        if (pend) {
+          const float2 d0 = dd[t], x0 = xx[t];
+          const float2 dn = cfma(eta, p, make_float2(kap * d0.x, kap * d0.y));
+          dd[t] = dn;
+          xx[t] = make_float2(fmaf(xmix, dn.x, x0.x), fmaf(xmix, dn.y, x0.y));
+        }
+      }
     }
-    wait_k(kb_);
-    const float *rk = RK + kb_ * 4 * kKN;
-    const float *re = RE + kb_ * 4 * kKN;
-    auto kks = [&](int c, int off) {
-      const float e = has_eps ? re[c * kKN + ck + off] : 1.0f;
-      return make_float2(-ka * e, kb * rk[c * kKN + ck + off]);
-    };
-    auto kkg = [&](int c, long long nd) {
-      const float e = has_eps ? __ldg(eps + c * N + nd) : 1.0f;
-      return make_float2(-ka * e, kb * __ldg(sig + c * N + nd));
-    };
+  };
+  auto halo = [&](int st, float2 *Us) {
+    const float2 *R = reinterpret_cast<const float2 *>(shm + st * kStage);
+    float2 vt;
+    Us[hc * kPN + he] = combine(R[hc * kPN + he], R[(4 + hc) * kPN + he], R[(8 + hc) * kPN + he], vt);
+  };
+
+  // per-thread axis coefficients
+  const int ic = min(i, nx - 1), jc = min(j, ny - 1);
+  const float4 *AX = D.ax32, *AY = D.ax32 + 2 * nx, *AZ = D.ax32 + 2 * (nx + ny);
+  const float4 XA = __ldg(AX + ic), XB = __ldg(AX + nx + ic), YA = __ldg(AY + jc), YB = __ldg(AY + ny + jc);
+  const bool hx = live && i < nx - 1, hy = live && j < ny - 1;
+  const bool pxy = live && i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
+
+  // ---- prologue: step k0-1
+  if (threadIdx.x == 0) {
+    issue(0, k0 - 1);
+    issue(1, k0);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) um[c] = make_float2(0.f, 0.f);
+  if (live && k0 > 0) {  // u of plane k0-1, own node: the first plane's z-neighbour
+    const float2 *Qr = wvec(D, cur, sys, 0), *Vr = wvec(D, cur, sys, 1), *Pr = wvec(D, cur, sys, 2);
+    const long long nd = ndc + (k0 - 1) * plane;
+    float2 vt;
+#pragma unroll
+    for (int c = 0; c < 4; c++) um[c] = combine(__ldg(Qr + c * N + nd), __ldg(Vr + c * N + nd), __ldg(Pr + c * N + nd), vt);
+  }
+  wait(0);
+  own_step(0, k0, Ub, uc, vc);
+  halo(0, Ub);
+  float s2m = reinterpret_cast<const float *>(shm + kRawBytes)[2 * kKN + ck];  // sigma-bar of Az at k0-1
+  float e2m = EPS ? reinterpret_cast<const float *>(shm + kRawBytes + kSigBytes)[2 * kKN + ck] : 1.f;
+  __syncthreads();
+  if (threadIdx.x == 0 && k0 + 1 <= k1 - 1) issue(0, k0 + 1);
+
+  double acc[kParts];
+#pragma unroll
+  for (int q = 0; q < kParts; q++) acc[q] = 0.0;
+
+  for (int m = k0; m < k1; m++) {
+    const int st = (m - k0 + 1) & 1;
+    const float2 *Uc = Ub + ((m - k0) & 1) * 4 * kPN;
+    float2 *Un = Ub + ((m - k0 + 1) & 1) * 4 * kPN;
+    const long long nd = ndc + m * plane;
+    float2 di[4];
+    float s3p = 0.f, e3p = 1.f;
+#pragma unroll
+    for (int c = 0; c < 4; c++) di[c] = make_float2(0.f, 0.f);
     if (live) {
-      const float2 *Um = U + ((k - 1 - k0 + 3) % 3) * 4 * kPN;
-      const float2 *Uc = U + ((k - k0 + 3) % 3) * 4 * kPN;
-      const float2 *Up = U + ((k + 1 - k0 + 3) % 3) * 4 * kPN;
-      const float zn4 = (float)Z.n4[k], zn5 = (float)Z.n5[k], dzc = (float)Z.dc[k];
-      const long long nd = ndc + k * plane;
-      const float2 kpc = kks(3, 0), phc = Uc[3 * kPN + c0];
+#pragma unroll
+      for (int c = 0; c < 4; c++) di[c] = __ldg(dv + c * N + nd);
+      if (m + 1 < nz) {
+        s3p = __ldg(sig + 3 * N + nd + plane);
+        if (EPS) e3p = __ldg(eps + 3 * N + nd + plane);
+      }
+    }
+    wait(st);
+    own_step(st, m + 1, Un, up, vn);
+
+    const float *rk = reinterpret_cast<const float *>(shm + st * kStage + kRawBytes);
+    const float *re = reinterpret_cast<const float *>(shm + st * kStage + kRawBytes + kSigBytes);
+    const float sx = rk[ck], sy = rk[kKN + ck], sz = rk[2 * kKN + ck], sp0 = rk[3 * kKN + ck];
+    const float ex = EPS ? re[ck] : 1.f, ey = EPS ? re[kKN + ck] : 1.f;
+    const float ez = EPS ? re[2 * kKN + ck] : 1.f, ep0 = EPS ? re[3 * kKN + ck] : 1.f;
+    if (live) {
+      const float4 ZA = __ldg(AZ + m), ZB = __ldg(AZ + nz + m);
+      const float xn4 = XA.x, xn5 = XA.y, dxc = XA.z, rdxc = XA.w, ce2x = XB.x, ce3x = XB.y, dxi = XB.z,
+                  rdxi = XB.w;
+      const float yn4 = YA.x, yn5 = YA.y, dyc = YA.z, rdyc = YA.w, ce2y = YB.x, ce3y = YB.y, dyj = YB.z,
+                  rdyj = YB.w;
+      const float zn4 = ZA.x, zn5 = ZA.y, dzc = ZA.z, rdzc = ZA.w, ce2z = ZB.x, ce3z = ZB.y, dzk = ZB.z,
+                  rdzk = ZB.w;
+      const float2 *U0 = Uc, *U1 = Uc + kPN, *U2 = Uc + 2 * kPN, *U3 = Uc + 3 * kPN;
       float2 w[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      // k^2 = (-ka e, kb s) of a component value
+      auto K2 = [&](float s, float e) { return make_float2(-ka * e, kb * s); };
       if (hx) {
         const float vol = dxi * dyc * dzc;
-        const float2 k2 = kks(0, 0), kp2 = kks(3, 1);
+        const float spx = rk[3 * kKN + ck + 1];
         const float sum = ce2x + ce3x + yn4 + yn5 + zn4 + zn5;
-        const float2 *u = Uc;
-        float2 t = cmul(make_float2(-sum + k2.x, k2.y), u[c0]);
-        t = cadd(t, rmul(ce2x, u[c0 + 1]));
-        t = cadd(t, rmul(ce3x, u[c0 - 1]));
-        t = cadd(t, rmul(yn4, u[c0 + kPW]));
-        t = cadd(t, rmul(yn5, u[c0 - kPW]));
-        t = cadd(t, rmul(zn4, Up[c0]));
-        t = cadd(t, rmul(zn5, Um[c0]));
-        const float2 gr = rdiv(csub(cmul(Uc[3 * kPN + c0 + 1], csub(kp2, k2)), cmul(phc, csub(kpc, k2))), dxi);
-        w[0] = rmul(vol, cadd(t, gr));
+        float2 L = axpy(ce2x, U0[eo + 1], make_float2(0.f, 0.f));
+        L = axpy(ce3x, U0[eo - 1], L);
+        L = axpy(yn4, U0[eo + kPW], L);
+        L = axpy(yn5, U0[eo - kPW], L);
+        L = axpy(zn4, up[0], L);
+        L = axpy(zn5, um[0], L);
+        if (!EPS) {
+          L = axpy(-sum - ka, uc[0], L);
+          float2 Mv = make_float2(sx * uc[0].x, sx * uc[0].y);
+          Mv = axpy(rdxi * (spx - sx), U3[eo + 1], Mv);
+          Mv = axpy(-rdxi * (sp0 - sx), uc[3], Mv);
+          w[0] = make_float2(vol * (L.x - kb * Mv.y), vol * (L.y + kb * Mv.x));
+        } else {
+          const float2 k2 = K2(sx, ex), kpx = K2(spx, re[3 * kKN + ck + 1]), kp0 = K2(sp0, ep0);
+          L = cfma(make_float2(-sum + k2.x, k2.y), uc[0], L);
+          L = cfma(make_float2(rdxi * (kpx.x - k2.x), rdxi * (kpx.y - k2.y)), U3[eo + 1], L);
+          L = cfma(make_float2(-rdxi * (kp0.x - k2.x), -rdxi * (kp0.y - k2.y)), uc[3], L);
+          w[0] = make_float2(vol * L.x, vol * L.y);
+        }
       }
       if (hy) {
         const float vol = dxc * dyj * dzc;
-        const float2 k2 = kks(1, 0), kp2 = kks(3, kKW);
+        const float spy = rk[3 * kKN + ck + kKW];
         const float sum = ce2y + ce3y + xn4 + xn5 + zn4 + zn5;
-        const float2 *u = Uc + kPN;
-        float2 t = cmul(make_float2(-sum + k2.x, k2.y), u[c0]);
-        t = cadd(t, rmul(ce2y, u[c0 + kPW]));
-        t = cadd(t, rmul(ce3y, u[c0 - kPW]));
-        t = cadd(t, rmul(xn4, u[c0 + 1]));
-        t = cadd(t, rmul(xn5, u[c0 - 1]));
-        t = cadd(t, rmul(zn4, Up[kPN + c0]));
-        t = cadd(t, rmul(zn5, Um[kPN + c0]));
-        const float2 gr = rdiv(csub(cmul(Uc[3 * kPN + c0 + kPW], csub(kp2, k2)), cmul(phc, csub(kpc, k2))), dyj);
-        w[1] = rmul(vol, cadd(t, gr));
+        float2 L = axpy(ce2y, U1[eo + kPW], make_float2(0.f, 0.f));
+        L = axpy(ce3y, U1[eo - kPW], L);
+        L = axpy(xn4, U1[eo + 1], L);
+        L = axpy(xn5, U1[eo - 1], L);
+        L = axpy(zn4, up[1], L);
+        L = axpy(zn5, um[1], L);
+        if (!EPS) {
+          L = axpy(-sum - ka, uc[1], L);
+          float2 Mv = make_float2(sy * uc[1].x, sy * uc[1].y);
+          Mv = axpy(rdyj * (spy - sy), U3[eo + kPW], Mv);
+          Mv = axpy(-rdyj * (sp0 - sy), uc[3], Mv);
+          w[1] = make_float2(vol * (L.x - kb * Mv.y), vol * (L.y + kb * Mv.x));
+        } else {
+          const float2 k2 = K2(sy, ey), kpy = K2(spy, re[3 * kKN + ck + kKW]), kp0 = K2(sp0, ep0);
+          L = cfma(make_float2(-sum + k2.x, k2.y), uc[1], L);
+          L = cfma(make_float2(rdyj * (kpy.x - k2.x), rdyj * (kpy.y - k2.y)), U3[eo + kPW], L);
+          L = cfma(make_float2(-rdyj * (kp0.x - k2.x), -rdyj * (kp0.y - k2.y)), uc[3], L);
+          w[1] = make_float2(vol * L.x, vol * L.y);
+        }
       }
-      if (k < nz - 1) {
-        const float c2 = (float)Z.e2[k], c3 = (float)Z.e3[k], dzk = (float)Z.d[k + 1];
+      if (m < nz - 1) {
         const float vol = dxc * dyc * dzk;
-        const float2 k2 = kks(2, 0), kp2 = kkg(3, nd + plane);
-        const float sum = c2 + c3 + xn4 + xn5 + yn4 + yn5;
-        const float2 *u = Uc + 2 * kPN;
-        float2 t = cmul(make_float2(-sum + k2.x, k2.y), u[c0]);
-        t = cadd(t, rmul(c2, Up[2 * kPN + c0]));
-        t = cadd(t, rmul(c3, Um[2 * kPN + c0]));
-        t = cadd(t, rmul(xn4, u[c0 + 1]));
-        t = cadd(t, rmul(xn5, u[c0 - 1]));
-        t = cadd(t, rmul(yn4, u[c0 + kPW]));
-        t = cadd(t, rmul(yn5, u[c0 - kPW]));
-        const float2 gr = rdiv(csub(cmul(Up[3 * kPN + c0], csub(kp2, k2)), cmul(phc, csub(kpc, k2))), dzk);
-        w[2] = rmul(vol, cadd(t, gr));
+        const float sum = ce2z + ce3z + xn4 + xn5 + yn4 + yn5;
+        float2 L = axpy(ce2z, up[2], make_float2(0.f, 0.f));
+        L = axpy(ce3z, um[2], L);
+        L = axpy(xn4, U2[eo + 1], L);
+        L = axpy(xn5, U2[eo - 1], L);
+        L = axpy(yn4, U2[eo + kPW], L);
+        L = axpy(yn5, U2[eo - kPW], L);
+        if (!EPS) {
+          L = axpy(-sum - ka, uc[2], L);
+          float2 Mv = make_float2(sz * uc[2].x, sz * uc[2].y);
+          Mv = axpy(rdzk * (s3p - sz), up[3], Mv);
+          Mv = axpy(-rdzk * (sp0 - sz), uc[3], Mv);
+          w[2] = make_float2(vol * (L.x - kb * Mv.y), vol * (L.y + kb * Mv.x));
+        } else {
+          const float2 k2 = K2(sz, ez), kpz = K2(s3p, e3p), kp0 = K2(sp0, ep0);
+          L = cfma(make_float2(-sum + k2.x, k2.y), uc[2], L);
+          L = cfma(make_float2(rdzk * (kpz.x - k2.x), rdzk * (kpz.y - k2.y)), up[3], L);
+          L = cfma(make_float2(-rdzk * (kp0.x - k2.x), -rdzk * (kp0.y - k2.y)), uc[3], L);
+          w[2] = make_float2(vol * L.x, vol * L.y);
+        }
       }
-      if (pin && k > 0 && k < nz - 1) {
+      if (pxy && m > 0 && m < nz - 1) {
         const float vol = dxc * dyc * dzc;
-        const float2 s1 = kpc;
-        const float2 s2 = kks(0, 0), s3 = kks(0, -1), s4 = kks(1, 0), s5 = kks(1, -kKW);
-        const float2 s6 = kks(2, 0), s7 = kkg(2, nd - plane);
-        const float2 c2 = rmul(xn4, s2), c3 = rmul(xn5, s3), c4 = rmul(yn4, s4);
-        const float2 c5 = rmul(yn5, s5), c6 = rmul(zn4, s6), c7 = rmul(zn5, s7);
-        const float2 sum = cadd(cadd(cadd(cadd(cadd(c2, c3), c4), c5), c6), c7);
-        const float2 *u = Uc + 3 * kPN;
-        float2 t = cmul(cadd(cneg(sum), cmul(s1, s1)), phc);
-        t = cadd(t, cmul(c2, u[c0 + 1]));
-        t = cadd(t, cmul(c3, u[c0 - 1]));
-        t = cadd(t, cmul(c4, u[c0 + kPW]));
-        t = cadd(t, cmul(c5, u[c0 - kPW]));
-        t = cadd(t, cmul(c6, Up[3 * kPN + c0]));
-        t = cadd(t, cmul(c7, Um[3 * kPN + c0]));
-        float2 e = cmul(rdiv(csub(s2, s1), dxc), Uc[c0]);
-        e = cadd(e, cmul(cneg(rdiv(csub(s3, s1), dxc)), Uc[c0 - 1]));
-        e = cadd(e, cmul(rdiv(csub(s4, s1), dyc), Uc[kPN + c0]));
-        e = cadd(e, cmul(cneg(rdiv(csub(s5, s1), dyc)), Uc[kPN + c0 - kPW]));
-        e = cadd(e, cmul(rdiv(csub(s6, s1), dzc), Uc[2 * kPN + c0]));
-        e = cadd(e, cmul(cneg(rdiv(csub(s7, s1), dzc)), Um[2 * kPN + c0]));
-        w[3] = cadd(rmul(vol, t), rmul(vol, e));
+        const float sxm = rk[ck - 1], sym = rk[kKN + ck - kKW];
+        const float2 f1 = U3[eo + 1], f2 = U3[eo - 1], f3 = U3[eo + kPW], f4 = U3[eo - kPW];
+        const float2 a0m = U0[eo - 1], a1m = U1[eo - kPW];
+        if (!EPS) {
+          const float sn = xn4 + xn5 + yn4 + yn5 + zn4 + zn5;
+          const float ss = xn4 * sx + xn5 * sxm + yn4 * sy + yn5 * sym + zn4 * sz + zn5 * s2m;
+          float2 T1 = axpy(xn4, f1, make_float2(0.f, 0.f));
+          T1 = axpy(xn5, f2, T1);
+          T1 = axpy(yn4, f3, T1);
+          T1 = axpy(yn5, f4, T1);
+          T1 = axpy(zn4, up[3], T1);
+          T1 = axpy(zn5, um[3], T1);
+          float2 T2 = axpy(xn4 * sx, f1, make_float2(0.f, 0.f));
+          T2 = axpy(xn5 * sxm, f2, T2);
+          T2 = axpy(yn4 * sy, f3, T2);
+          T2 = axpy(yn5 * sym, f4, T2);
+          T2 = axpy(zn4 * sz, up[3], T2);
+          T2 = axpy(zn5 * s2m, um[3], T2);
+          T2 = axpy(rdxc * (sx - sp0), uc[0], T2);
+          T2 = axpy(-rdxc * (sxm - sp0), a0m, T2);
+          T2 = axpy(rdyc * (sy - sp0), uc[1], T2);
+          T2 = axpy(-rdyc * (sym - sp0), a1m, T2);
+          T2 = axpy(rdzc * (sz - sp0), uc[2], T2);
+          T2 = axpy(-rdzc * (s2m - sp0), um[2], T2);
+          const float dgr = ka * ka - kb * kb * sp0 * sp0 + ka * sn;
+          const float dgi = -2.f * ka * kb * sp0 - kb * ss;
+          const float2 t = cfma(make_float2(dgr, dgi), uc[3], make_float2(-ka * T1.x, -ka * T1.y));
+          w[3] = make_float2(vol * (t.x - kb * T2.y), vol * (t.y + kb * T2.x));
+        } else {
+          const float exm = re[ck - 1], eym = re[kKN + ck - kKW];
+          const float2 s1 = K2(sp0, ep0);
+          const float2 s2 = K2(sx, ex), s3 = K2(sxm, exm), s4 = K2(sy, ey), s5 = K2(sym, eym);
+          const float2 s6 = K2(sz, ez), s7 = K2(s2m, e2m);
+          const float2 c2 = make_float2(xn4 * s2.x, xn4 * s2.y), c3 = make_float2(xn5 * s3.x, xn5 * s3.y);
+          const float2 c4 = make_float2(yn4 * s4.x, yn4 * s4.y), c5 = make_float2(yn5 * s5.x, yn5 * s5.y);
+          const float2 c6 = make_float2(zn4 * s6.x, zn4 * s6.y), c7 = make_float2(zn5 * s7.x, zn5 * s7.y);
+          const float2 sum = make_float2(c2.x + c3.x + c4.x + c5.x + c6.x + c7.x, c2.y + c3.y + c4.y + c5.y + c6.y + c7.y);
+          const float2 s11 = cmul(s1, s1);
+          float2 t = cfma(make_float2(s11.x - sum.x, s11.y - sum.y), uc[3], make_float2(0.f, 0.f));
+          t = cfma(c2, f1, t);
+          t = cfma(c3, f2, t);
+          t = cfma(c4, f3, t);
+          t = cfma(c5, f4, t);
+          t = cfma(c6, up[3], t);
+          t = cfma(c7, um[3], t);
+          t = cfma(make_float2(rdxc * (s2.x - s1.x), rdxc * (s2.y - s1.y)), uc[0], t);
+          t = cfma(make_float2(-rdxc * (s3.x - s1.x), -rdxc * (s3.y - s1.y)), a0m, t);
+          t = cfma(make_float2(rdyc * (s4.x - s1.x), rdyc * (s4.y - s1.y)), uc[1], t);
+          t = cfma(make_float2(-rdyc * (s5.x - s1.x), -rdyc * (s5.y - s1.y)), a1m, t);
+          t = cfma(make_float2(rdzc * (s6.x - s1.x), rdzc * (s6.y - s1.y)), uc[2], t);
+          t = cfma(make_float2(-rdzc * (s7.x - s1.x), -rdzc * (s7.y - s1.y)), um[2], t);
+          w[3] = make_float2(vol * t.x, vol * t.y);
+        }
       }
-      float we_r = 0.f, we_i = 0.f;  // this node's share of u^T w
+      // q^ = D^-1 w; this node's shares of epsilon and of the six products
+      float r[kParts];
+#pragma unroll
+      for (int q = 0; q < kParts; q++) r[q] = 0.f;
 #pragma unroll
       for (int c = 0; c < 4; c++) {
-        const float2 sc = __ldg(sv + c * N + nd);
-        q[c * N + nd] = cmul(sc, w[c]);
-        const float2 e = cmul(Uc[c * kPN + c0], w[c]);
-        we_r += e.x;
-        we_i += e.y;
+        const float2 d = di[c], ww = w[c], u = uc[c], v = vc[c];
+        const float2 qh = cmul(d, ww);
+        Qw[c * N + nd] = qh;
+        const float m2 = d.x * d.x + d.y * d.y;
+        const float rs = m2 > 0.f ? rsqrtf(m2) : 0.f;  // |D|
+        const float mag = m2 * rs;                      // |D^-1|
+        r[0] += u.x * ww.x - u.y * ww.y;                // epsilon = u^T K u
+        r[1] += u.x * ww.y + u.y * ww.x;
+        r[2] += mag * (ww.x * ww.x + ww.y * ww.y);      // ||q~||^2
+        r[3] += rs * (v.x * qh.x + v.y * qh.y);         // v~^H q~
+        r[4] += rs * (v.x * qh.y - v.y * qh.x);
+        r[5] += rs * (v.x * v.x + v.y * v.y);           // ||v~||^2
+        r[6] += ww.x * qh.x - ww.y * qh.y;              // q~^T q~
+        r[7] += ww.x * qh.y + ww.y * qh.x;
+        r[8] += ww.x * v.x - ww.y * v.y;                // v~^T q~
+        r[9] += ww.x * v.y + ww.y * v.x;
+        const float v2r = v.x * v.x - v.y * v.y, v2i = 2.f * v.x * v.y, rs2 = rs * rs;
+        r[10] += rs2 * (v2r * d.x + v2i * d.y);         // v~^T v~ = sum v^2 conj(D^-1) / |D^-1|^2
+        r[11] += rs2 * (v2i * d.x - v2r * d.y);
       }
-      ea += (double)we_r;
-      eb += (double)we_i;
+#pragma unroll
+      for (int q = 0; q < kParts; q++) acc[q] += (double)r[q];
     }
-    if (more) wait_raw();  // plane k+2 has landed
-    __syncthreads();       // everyone is done with ring slot k-1 and the raw plane
-    if (more) {
-      convert(k + 2);
-      __syncthreads();
+    if (m + 1 < k1) halo(st, Un);
+    __syncthreads();  // everyone is done with stage st and with u plane m
+    if (threadIdx.x == 0 && m + 2 <= k1 - 1) issue(st, m + 2);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      um[c] = uc[c];
+      uc[c] = up[c];
+      vc[c] = vn[c];
     }
+    s2m = sz;
+    e2m = ez;
   }
 
-  Vals<2> blk = block_reduce<2, kPThreads>(Vals<2>{{ea, eb}});
-  double *part = D.part + (size_t)sys * D.slots * 6;
-  unsigned *cnt = D.cnt + CNT_APPLY * D.nsys + sys;
+  Vals<kParts> blk;
+#pragma unroll
+  for (int q = 0; q < kParts; q++) blk.v[q] = acc[q];
+  blk = block_reduce<kParts, kPThreads>(blk);
+  double *part = D.part + (size_t)sys * D.slots * kParts;
+  unsigned *cnt = D.cnt + CNT_PASS * D.nsys + sys;
   const unsigned nt = (unsigned)D.tp.count();
-  if (arrive<2, kPThreads>(blk, part, cnt, (unsigned)tile, nt)) {
-    Vals<2> tot = final_reduce<2, kPThreads>(part, cnt, nt);
-    if (SCALARS && threadIdx.x == 0) {
-      const double2 e = make_double2(tot.v[0], tot.v[1]);
-      S->eps = e;
-      if (!finite2(e) || zero2(e)) {  // breakdown: restart from the current x
-        S->phase = PH_OUTER;
-        return;
-      }
-      S->beta = cdiv(e, S->del);
-    }
-  }
-}
-
-// B: p~_n stored; vt = q~_n - beta_n v~_n stored unnormalised; the lagged
-// d~, x~ update of the previous iteration; ||vt||^2 and vt^T vt reduced,
-// then rho_{n+1}, delta_{n+1}, theta, c, eta, kappa, the quasi-residual and
-// the inner stop test (src/aphid_qmr.f90:332-390).  Two complex64 values per
-// 16-byte access over the node-layout vectors (pads and absent components
-// are zero and stay zero).
-static __global__ void __launch_bounds__(kStreamThreads) k_sw_update(SweepDev D) {
-  const int sys = blockIdx.x % D.nsys, chunk = blockIdx.x / D.nsys;
-  SweepSys *S = D.sys + sys;
-  if (S->phase != PH_INNER) return;
-  const long long vb = (long long)sys * 4 * D.L.N;
-  const float2 k1 = to_f(S->k1), beta = to_f(S->beta);
-  const float vsc = (float)S->vscale;
-  const bool pend = S->pending != 0;
-  const float2 eta = to_f(S->eta_pend);
-  const float kap = (float)S->kap_pend;
-  float4 *v = reinterpret_cast<float4 *>(D.v + vb), *p = reinterpret_cast<float4 *>(D.p + vb);
-  float4 *d = reinterpret_cast<float4 *>(D.d + vb), *x = reinterpret_cast<float4 *>(D.x + vb);
-  const float4 *q = reinterpret_cast<const float4 *>(D.q + vb);
-  const long long n2 = 2 * D.L.N;  // float4 count: 4N complex values / 2
-  Vals<3> a{{0.0, 0.0, 0.0}};
-  auto one = [&](float2 vt_old, float2 po, float2 qq, float2 &pn, float2 &vt) {
-    const float2 vn = vn32(vt_old, vsc);
-    pn = pnew32(vn, po, k1);
-    vt = csub(qq, cmul(beta, vn));
-    const double2 dv = to_d(vt);
-    a.v[0] += cabs2(dv);
-    a.v[1] += dv.x * dv.x - dv.y * dv.y;
-    a.v[2] += 2.0 * dv.x * dv.y;
-  };
-  for (long long t = chunk * (long long)blockDim.x + threadIdx.x; t < n2; t += (long long)D.bps * blockDim.x) {
-    const float4 v4 = v[t], p4 = p[t], q4 = q[t];
-    float2 pa, pb, va, vb2;
-    one(make_float2(v4.x, v4.y), make_float2(p4.x, p4.y), make_float2(q4.x, q4.y), pa, va);
-    one(make_float2(v4.z, v4.w), make_float2(p4.z, p4.w), make_float2(q4.z, q4.w), pb, vb2);
-    p[t] = make_float4(pa.x, pa.y, pb.x, pb.y);
-    v[t] = make_float4(va.x, va.y, vb2.x, vb2.y);
-    if (pend) {
-      const float4 d4 = d[t], x4 = x[t];
-      const float2 da = cadd(cmul(eta, make_float2(p4.x, p4.y)), rmul(kap, make_float2(d4.x, d4.y)));
-      const float2 db = cadd(cmul(eta, make_float2(p4.z, p4.w)), rmul(kap, make_float2(d4.z, d4.w)));
-      d[t] = make_float4(da.x, da.y, db.x, db.y);
-      x[t] = make_float4(x4.x + da.x, x4.y + da.y, x4.z + db.x, x4.w + db.y);
-    }
-  }
-  Vals<3> blk = block_reduce<3, kStreamThreads>(a);
-  double *part = D.part + (size_t)sys * D.slots * 6;
-  unsigned *cnt = D.cnt + CNT_UPDATE * D.nsys + sys;
-  if (arrive<3, kStreamThreads>(blk, part, cnt, chunk, D.bps)) {
-    Vals<3> tot = final_reduce<3, kStreamThreads>(part, cnt, D.bps);
+  if (arrive<kParts, kPThreads>(blk, part, cnt, (unsigned)tile, nt)) {
+    Vals<kParts> tot = final_reduce<kParts, kPThreads>(part, cnt, nt);
     if (threadIdx.x == 0) {
-      S->inner_it++;
-      S->total_it++;
-      // from here on p~_n is stored and the previous lagged update is applied
-      const double rho = sqrt(tot.v[0]);
-      const double2 beta_d = S->beta;
-      if (!(rho > 0.0) || !isfinite(rho)) {  // Krylov space exhausted
-        S->pending = 0;
-        S->phase = PH_OUTER;
-        return;
-      }
-      S->rho_np = rho;
-      S->theta_n = rho * rho / S->c_nm / (beta_d.x * beta_d.x + beta_d.y * beta_d.y);
-      S->c_n = 1.0 / (1.0 + S->theta_n);
-      S->eta = cdiv(rmul(S->c_n, rmul(S->rho_n, cneg(S->eta))), rmul(S->c_nm, beta_d));
-      S->kap = S->theta_nm * S->c_n;
-      S->tau = S->tau * sqrt(S->theta_n * S->c_n);
-      S->eta_pend = S->eta;
-      S->kap_pend = S->kap;
-      S->pending = 1;
-      S->vscale = 1.0 / rho;
-      const double2 del = rmul(1.0 / (rho * rho), make_double2(tot.v[1], tot.v[2]));
-      if (!finite2(S->eta) || !isfinite(S->tau) || !finite2(del) || zero2(del) ||
-          S->tau < S->inner_tol * S->tau0 || S->total_it >= S->max_it) {
-        S->phase = PH_OUTER;
-        return;
-      }
-      S->c_nm = S->c_n;
-      S->rho_n = rho;
-      S->theta_nm = S->theta_n;
-      S->del = del;
-      S->k1 = cdiv(rmul(S->rho_n, del), S->eps);
+      if (TIMING)
+        S->cur ^= 1;
+      else
+        pass_scalars(S, tot.v);
     }
   }
 }

@@ -224,11 +224,13 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega,
 /* Copy system `sys` of the last sweep into x (one [x|y|z|p] vector). */
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);
 
-/* Benchmarking hook, no counterpart in the reference: launch the complex64
- * operator pass of the inner QMR (q~ = D^-1/2 K D^-1/2 p~ with its epsilon
- * and rho sums) `reps` times over all systems of the last mixed-precision
- * sweep, on the context's stream, without the scalar recurrence, so no system
- * changes state.  Returns after the launches (asynchronous). */
+/* Benchmarking hook, no counterpart in the reference: launch the fused
+ * complex64 QMR iteration pass (p update, q^ = D^-1 K p^, the lagged d/x
+ * update with zero weights, the inner products) `reps` times over all
+ * systems of the last mixed-precision sweep, on the context's stream, without
+ * the scalar recurrence.  The solutions (aphid_gpu_sweep_fetch) are not
+ * changed; the inner Krylov vectors are, as by an iteration.  Returns after
+ * the launches (asynchronous). */
 int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps);
 
 /* ---- allocation-free operator apply -------------------------------------- */
