@@ -68,8 +68,10 @@ struct aphid_ctx {
   int sw_nsys = 0;           // systems the buffers hold
   bool sw_f32_ok = false;    // complex64 vectors allocated
   double2 *sw_f64 = nullptr; // [2][nsys][n]: x64, b
-  float2 *sw_f32 = nullptr;  // [9][nsys][4][N]: 2 sets of q^ v^ p^, then d^ x^ D^-1 (node layout)
+  float2 *sw_f32 = nullptr;  // [8][nsys][4][N]: 2 sets of q^ v^ p^, then d^ x^ (node layout)
   float4 *sw_ax32 = nullptr; // FP32 axis tables of the complex64 pass
+  int *sw_work = nullptr;    // [2] work counter of the persistent pass, then [order]
+  int num_sms = 148;         // multiprocessors of the device
   PassMaps maps{};           // TMA tensor maps of the pass
   int *sw_err = nullptr;     // set by a kernel whose bounded wait gave up
   SweepSys *sw_sys = nullptr;
@@ -140,6 +142,8 @@ void release_work(aphid_ctx *ctx) {
   cudaFree(ctx->sw_f32);
   cudaFree(ctx->sw_ax32);
   ctx->sw_ax32 = nullptr;
+  cudaFree(ctx->sw_work);
+  ctx->sw_work = nullptr;
   cudaFree(ctx->sw_sys);
   cudaFree(ctx->sw_part);
   cudaFree(ctx->sw_cnt);
@@ -270,6 +274,7 @@ int aphid_gpu_create(aphid_ctx **out, const aphid_opts *opts) {
     delete ctx;
     return APHID_ERR_NODEVICE;  // kernels are built for sm_100a only
   }
+  ctx->num_sms = prop.multiProcessorCount;
   if (cudaSetDevice(ctx->device) != cudaSuccess) {
     delete ctx;
     return APHID_ERR_NODEVICE;
@@ -710,7 +715,21 @@ int vector_maps(aphid_ctx *ctx) {
   const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * 8, (cuuint64_t)L.nxp * ctx->ny * 8, (cuuint64_t)L.N * 8,
                                  (cuuint64_t)L.N * 96};
   const cuuint32_t box[5] = {kPW, kPH, 1, 12, 1};
-  return encode_map(ctx, &ctx->maps.w, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32, dims, strides, box);
+  int rc = encode_map(ctx, &ctx->maps.w, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32, dims, strides, box);
+  if (rc) return rc;
+  // d^, x^: 5-D (i, j, k, component, system); one box = the 16 x 16 tile of
+  // one z-plane, four components
+  const size_t v32 = (size_t)ctx->sw_nsys * 4 * L.N;
+  const cuuint64_t odims[5] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4,
+                               (cuuint64_t)ctx->sw_nsys};
+  const cuuint64_t ostrides[4] = {(cuuint64_t)L.nxp * 8, (cuuint64_t)L.nxp * ctx->ny * 8, (cuuint64_t)L.N * 8,
+                                  (cuuint64_t)L.N * 32};
+  const cuuint32_t obox[5] = {kPTI, kPTJ, 1, 4, 1};
+  if ((rc = encode_map(ctx, &ctx->maps.dd, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + 6 * v32, odims,
+                       ostrides, obox)))
+    return rc;
+  return encode_map(ctx, &ctx->maps.xx, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + 7 * v32, odims, ostrides,
+                    obox);
 }
 
 // sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18
@@ -743,13 +762,14 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   D.L = ctx->nl;
   D.err = ctx->sw_err;
   D.tmix = 1.f;
+  D.work = ctx->sw_work;
+  D.order = ctx->sw_work ? ctx->sw_work + 2 : nullptr;
   const size_t vec = (size_t)ctx->sw_nsys * ctx->n;
   const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
   if (ctx->sw_f32_ok) {
     D.W = ctx->sw_f32;
     D.dd = ctx->sw_f32 + 6 * v32;
     D.xx = ctx->sw_f32 + 7 * v32;
-    D.dinv = ctx->sw_f32 + 8 * v32;
     D.ax32 = ctx->sw_ax32;
   }
   D.x64 = ctx->sw_f64;
@@ -796,6 +816,27 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     tp.tk = (ctx->nz + tp.kz - 1) / tp.kz;
     ctx->ptiles = tp;
     ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()), tp.count());
+    // work counter and the order in which the pass takes its tiles: most
+    // live nodes first, so that the tiles at the far x and y faces (one live
+    // column or row on meshes of 16k+1 nodes) fill the tail
+    {
+      const long long T = tp.count();
+      std::vector<int> order(T);
+      std::vector<long long> live(T);
+      for (long long t = 0; t < T; t++) {
+        order[t] = (int)t;
+        const int bi = (int)(t % tp.ti), bj = (int)((t / tp.ti) % tp.tj), bk = (int)(t / ((long long)tp.ti * tp.tj));
+        const long long li = std::min(kPTI, ctx->nx - bi * kPTI), lj = std::min(kPTJ, ctx->ny - bj * kPTJ);
+        const long long lk = std::min(tp.kz, ctx->nz - bk * tp.kz);
+        live[t] = li * lj * lk;
+      }
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return live[a] > live[b]; });
+      cudaFree(ctx->sw_work);
+      ctx->sw_work = nullptr;
+      CK(cudaMalloc(&ctx->sw_work, (2 + T) * sizeof(int)));
+      CK(cudaMemset(ctx->sw_work, 0, 2 * sizeof(int)));
+      CK(cudaMemcpy(ctx->sw_work + 2, order.data(), T * sizeof(int), cudaMemcpyHostToDevice));
+    }
     CK(cudaMalloc(&ctx->sw_sys, (size_t)nsys * sizeof(SweepSys)));
     CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * kParts * sizeof(double)));
     CK(cudaMalloc(&ctx->sw_cnt, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
@@ -805,13 +846,13 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
   }
   if (mixed && !ctx->sw_f32_ok) {
     const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
-    if (cudaMalloc(&ctx->sw_f32, 9 * v32 * sizeof(float2)) != cudaSuccess) {
+    if (cudaMalloc(&ctx->sw_f32, 8 * v32 * sizeof(float2)) != cudaSuccess) {
       cudaGetLastError();
       ctx->sw_f32 = nullptr;
       return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex64 vectors failed");
     }
     // pads and components that do not exist stay zero for good
-    CK(cudaMemset(ctx->sw_f32, 0, 9 * v32 * sizeof(float2)));
+    CK(cudaMemset(ctx->sw_f32, 0, 8 * v32 * sizeof(float2)));
     if (!ctx->sw_ax32) {
       CK(cudaMalloc(&ctx->sw_ax32, 2 * (size_t)(ctx->nx + ctx->ny + ctx->nz) * sizeof(float4)));
       const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));
@@ -879,8 +920,10 @@ int pass_attrs(aphid_ctx *ctx) {
   return APHID_OK;
 }
 
+// persistent: one block per SM
 void launch_pass(aphid_ctx *ctx, const SweepDev &D, bool timing) {
-  const unsigned sp = (unsigned)(D.tp.count() * D.nsys);
+  const long long items = D.tp.count() * D.nsys;
+  const unsigned sp = (unsigned)std::min<long long>(items, (long long)ctx->num_sms);
   const size_t shm = pass_shm(D);
   if (D.epsr32) {
     if (timing)
@@ -1058,10 +1101,8 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
 
   if (mixed) {
     k_sw_bnorm<<<(unsigned)(D.bps * nsys), kStreamThreads, 0, ctx->stream>>>(D);
-    const dim3 sg((unsigned)((ctx->nx + 127) / 128), (unsigned)ctx->ny, (unsigned)(ctx->nz * nsys));
-    k_sw_dinv<<<sg, 128, 0, ctx->stream>>>(D);
     CK(cudaGetLastError());
-    nlaunch += 2;
+    nlaunch += 1;
     if ((rc = sweep_graph(ctx, D))) return rc;
     const long long per_round = 3 + (long long)ctx->graph_iters;
     const long long max_rounds = (long long)std::max(1, opts->max_it) / ctx->graph_iters + 2LL * (hs[0].max_outer + 2);

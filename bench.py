@@ -151,9 +151,10 @@ def run_reference(args):
 
 def pass_bytes(nsys, n):
     """Algorithmic bytes of one fused complex64 QMR pass over a batch: per
-    unknown and system read q^, v^, p^, D^-1, d^, x^ and write q^, v^, p^,
-    d^, x^ (11 x 8 B), plus the shared FP32 sigma-bar once (4 B)."""
-    return nsys * n * 88 + n * 4
+    unknown and system read q^, v^, p^, d^, x^ and write q^, v^, p^, d^, x^
+    (10 x 8 B; the Jacobi diagonal is formed on chip), plus the shared FP32
+    sigma-bar once (4 B)."""
+    return nsys * n * 80 + n * 4
 
 
 def time_apply(s, k2, n, dev, stream, reps=50):
