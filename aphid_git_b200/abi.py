@@ -87,6 +87,7 @@ def load():
                                   C.POINTER(SweepOpts), P, P]
     L.aphid_gpu_sweep_fetch.argtypes = [P, C.c_int, P]
     L.aphid_gpu_sweep_time_apply.argtypes = [P, C.c_int]
+    L.aphid_gpu_sweep_plane_kz.argtypes = [P]
     _lib = L
     return L
 
@@ -303,9 +304,15 @@ class Solver:
         return X, [i.as_dict() for i in infos]
 
     def sweep_time_apply(self, reps):
-        """Launch the complex64 operator pass `reps` times on the resident
-        systems of the last mixed sweep (asynchronous; for timing)."""
+        """Launch the fused complex64 QMR pass `reps` times on the resident
+        systems of the last mixed sweep (asynchronous; for timing; the
+        solutions are not changed)."""
         self._check(self.lib.aphid_gpu_sweep_time_apply(self._h, int(reps)), "sweep_time_apply")
+
+    def sweep_plane_kz(self):
+        """z-planes per work item of the complex64 pass in use (the
+        autotuner's choice unless plane_kz was fixed); 0 before a mixed sweep."""
+        return int(self.lib.aphid_gpu_sweep_plane_kz(self._h))
 
     def sweep_fetch(self, sys):
         x = np.empty(self.n, np.complex128)

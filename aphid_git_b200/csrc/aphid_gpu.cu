@@ -7,6 +7,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <cstdlib>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -781,6 +784,48 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   return D;
 }
 
+constexpr int kMinKz = 4;  // shallowest z-slab of the complex64 pass
+
+// z-slab depth when neither the caller nor the tuner chose one: about two
+// work items per SM over the whole batch
+int default_kz(const aphid_ctx *ctx, int nsys) {
+  const long long cols = (long long)((ctx->nx + kPTI - 1) / kPTI) * ((ctx->ny + kPTJ - 1) / kPTJ) * nsys;
+  return (int)std::min<long long>(32, std::max<long long>(kMinKz, cols * ctx->nz / (2LL * ctx->num_sms)));
+}
+
+// plane tiles of the complex64 pass for z-slab depth kz, the work counter
+// and the order in which the pass takes its tiles: most live nodes first, so
+// that the tiles at the far x and y faces (one live column or row on meshes
+// of 16k+1 nodes) fill the tail
+int plane_tiles(aphid_ctx *ctx, int kz) {
+  Tiles tp;
+  tp.ti = (ctx->nx + kPTI - 1) / kPTI;
+  tp.tj = (ctx->ny + kPTJ - 1) / kPTJ;
+  tp.kz = std::max(kMinKz, std::min(kz, ctx->nz));
+  tp.tk = (ctx->nz + tp.kz - 1) / tp.kz;
+  const long long T = tp.count();
+  std::vector<int> order(T);
+  std::vector<long long> live(T);
+  for (long long t = 0; t < T; t++) {
+    order[t] = (int)t;
+    const int bi = (int)(t % tp.ti), bj = (int)((t / tp.ti) % tp.tj), bk = (int)(t / ((long long)tp.ti * tp.tj));
+    const long long li = std::min(kPTI, ctx->nx - bi * kPTI), lj = std::min(kPTJ, ctx->ny - bj * kPTJ);
+    const long long lk = std::min(tp.kz, ctx->nz - bk * tp.kz);
+    live[t] = li * lj * lk;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return live[a] > live[b]; });
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(ctx->sw_work);
+  ctx->sw_work = nullptr;
+  CK(cudaMalloc(&ctx->sw_work, (2 + T) * sizeof(int)));
+  CK(cudaMemset(ctx->sw_work, 0, 2 * sizeof(int)));
+  CK(cudaMemcpy(ctx->sw_work + 2, order.data(), T * sizeof(int), cudaMemcpyHostToDevice));
+  ctx->ptiles = tp;
+  return APHID_OK;
+}
+
 int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
   const bool grow = nsys > ctx->sw_nsys;
   if (grow || (mixed && !ctx->sw_f32_ok)) {
@@ -805,38 +850,15 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     }
     ctx->sw_bps = (int)std::max<long long>(
         1, std::min<long long>((ctx->n + kStreamThreads - 1) / kStreamThreads, std::max(4, 148 * 8 / nsys)));
-    // plane tiles: about 2 waves of 148 SMs x 2 blocks over the whole batch
-    Tiles tp;
-    tp.ti = (ctx->nx + kPTI - 1) / kPTI;
-    tp.tj = (ctx->ny + kPTJ - 1) / kPTJ;
-    const long long cols = (long long)tp.ti * tp.tj * nsys;
-    tp.kz = ctx->plane_kz > 0
-                ? ctx->plane_kz
-                : (int)std::min<long long>(32, std::max<long long>(4, cols * ctx->nz / (148 * 2 * 2)));
-    tp.tk = (ctx->nz + tp.kz - 1) / tp.kz;
-    ctx->ptiles = tp;
-    ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()), tp.count());
-    // work counter and the order in which the pass takes its tiles: most
-    // live nodes first, so that the tiles at the far x and y faces (one live
-    // column or row on meshes of 16k+1 nodes) fill the tail
-    {
-      const long long T = tp.count();
-      std::vector<int> order(T);
-      std::vector<long long> live(T);
-      for (long long t = 0; t < T; t++) {
-        order[t] = (int)t;
-        const int bi = (int)(t % tp.ti), bj = (int)((t / tp.ti) % tp.tj), bk = (int)(t / ((long long)tp.ti * tp.tj));
-        const long long li = std::min(kPTI, ctx->nx - bi * kPTI), lj = std::min(kPTJ, ctx->ny - bj * kPTJ);
-        const long long lk = std::min(tp.kz, ctx->nz - bk * tp.kz);
-        live[t] = li * lj * lk;
-      }
-      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return live[a] > live[b]; });
-      cudaFree(ctx->sw_work);
-      ctx->sw_work = nullptr;
-      CK(cudaMalloc(&ctx->sw_work, (2 + T) * sizeof(int)));
-      CK(cudaMemset(ctx->sw_work, 0, 2 * sizeof(int)));
-      CK(cudaMemcpy(ctx->sw_work + 2, order.data(), T * sizeof(int), cudaMemcpyHostToDevice));
-    }
+    // partial-sum slots for the shallowest slab the tuner may choose
+    Tiles t4;
+    t4.ti = (ctx->nx + kPTI - 1) / kPTI;
+    t4.tj = (ctx->ny + kPTJ - 1) / kPTJ;
+    t4.kz = kMinKz;
+    t4.tk = (ctx->nz + kMinKz - 1) / kMinKz;
+    ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()), t4.count());
+    int rc = plane_tiles(ctx, ctx->plane_kz > 0 ? ctx->plane_kz : default_kz(ctx, nsys));
+    if (rc) return rc;
     CK(cudaMalloc(&ctx->sw_sys, (size_t)nsys * sizeof(SweepSys)));
     CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * kParts * sizeof(double)));
     CK(cudaMalloc(&ctx->sw_cnt, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
@@ -964,6 +986,101 @@ int sweep_graph(aphid_ctx *ctx, const SweepDev &D) {
   return APHID_OK;
 }
 
+// ------------------------------------------------------------- autotuner
+// The z-slab depth of the complex64 pass is chosen by timing the pass itself
+// (timing launches over the resident buffers, which leave the solver state
+// alone) for each candidate depth on this mesh and batch, and cached per
+// (mesh, batch, model kind) in the process and, when the environment
+// variable APHID_TUNE_CACHE names a file, across processes (one line
+// "nx ny nz nsys eps kz" per shape).
+typedef std::array<int, 5> TuneKey;  // nx, ny, nz, nsys, eps-bar present
+
+std::mutex &tune_mutex() {
+  static std::mutex m;
+  return m;
+}
+std::map<TuneKey, int> &tune_cache() {
+  static std::map<TuneKey, int> m;
+  return m;
+}
+
+int tune_file_lookup(const TuneKey &k) {
+  const char *path = std::getenv("APHID_TUNE_CACHE");
+  if (!path || !*path) return 0;
+  FILE *f = std::fopen(path, "r");
+  if (!f) return 0;
+  int v[6], found = 0;
+  while (std::fscanf(f, "%d %d %d %d %d %d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) == 6)
+    if (v[0] == k[0] && v[1] == k[1] && v[2] == k[2] && v[3] == k[3] && v[4] == k[4] && v[5] >= kMinKz) found = v[5];
+  std::fclose(f);
+  return found;
+}
+
+void tune_file_store(const TuneKey &k, int kz) {
+  const char *path = std::getenv("APHID_TUNE_CACHE");
+  if (!path || !*path) return;
+  FILE *f = std::fopen(path, "a");
+  if (!f) return;
+  std::fprintf(f, "%d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4], kz);
+  std::fclose(f);
+}
+
+int tune_kz(aphid_ctx *ctx, int nsys) {
+  const TuneKey key = {ctx->nx, ctx->ny, ctx->nz, nsys, ctx->d_epsr32 ? 1 : 0};
+  int kz = 0;
+  {
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) kz = it->second;
+  }
+  if (!kz) kz = tune_file_lookup(key);
+  int rc;
+  if (!kz) {
+    int rc0 = pass_attrs(ctx);
+    if (rc0) return rc0;
+    CK(cudaMemsetAsync(ctx->sw_sys, 0, (size_t)nsys * sizeof(SweepSys), ctx->stream));
+    CK(cudaMemsetAsync(ctx->sw_err, 0, sizeof(int), ctx->stream));
+    float best_ms = 0.f;
+    const int cand[] = {4, 6, 8, 12, 16, 24, 32};
+    int last_tk = -1;
+    for (int c : cand) {
+      if (c > ctx->nz) break;
+      const int tk = (ctx->nz + c - 1) / c;
+      if (tk == last_tk) continue;  // same slabs as the previous candidate
+      last_tk = tk;
+      if ((rc = plane_tiles(ctx, c))) return rc;
+      SweepDev D = sweep_dev(ctx, nsys);
+      D.tmix = 0.f;
+      for (int r = 0; r < 2; r++) launch_pass(ctx, D, true);
+      CK(cudaEventRecord(ctx->ev0, ctx->stream));
+      for (int r = 0; r < 5; r++) launch_pass(ctx, D, true);
+      CK(cudaEventRecord(ctx->ev1, ctx->stream));
+      CK(cudaEventSynchronize(ctx->ev1));
+      CK(cudaGetLastError());
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+      if (!kz || ms < best_ms) {
+        kz = c;
+        best_ms = ms;
+      }
+      if (ctx->verbose) std::fprintf(stderr, "aphid_gpu: tune kz=%d %.3f ms/pass\n", c, ms / 5);
+    }
+    int kerr = 0;
+    CK(cudaMemcpy(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (kerr) return fail(ctx, APHID_ERR_CUDA, "tuner: a tensor-copy wait in the pass timed out");
+    if (!kz) kz = default_kz(ctx, nsys);
+    tune_file_store(key, kz);
+  }
+  {
+    std::lock_guard<std::mutex> lock(tune_mutex());
+    tune_cache()[key] = kz;
+  }
+  if (ctx->ptiles.kz != kz || !ctx->sw_work) {
+    if ((rc = plane_tiles(ctx, kz))) return rc;
+  }
+  return APHID_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1044,10 +1161,16 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
   if (!(opts->target >= 0.0) || opts->max_it < 0) return fail(ctx, APHID_ERR_BADARG, "bad target or max_it");
   if (mixed && 4 * ctx->nl.N >= (1LL << 31))
     return fail(ctx, APHID_ERR_BADARG, "mixed sweep: more than 2^31 node-layout values per system");
-  if (mixed && (long long)ctx->nz * nsys > 65535)
-    return fail(ctx, APHID_ERR_BADARG, "nz * nsys exceeds the launch grid; split the sweep");
   if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
   if ((rc = ensure_work(ctx))) return rc;
+  if (mixed) {
+    if (ctx->plane_kz > 0) {
+      if (ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) && (rc = plane_tiles(ctx, ctx->plane_kz)))
+        return rc;
+    } else if ((rc = tune_kz(ctx, nsys))) {
+      return rc;
+    }
+  }
 
   // sources -> sparse right-hand sides
   std::vector<std::map<long long, double>> src;
@@ -1183,6 +1306,11 @@ int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {
   for (int r = 0; r < reps; r++) launch_pass(ctx, D, true);
   CK(cudaGetLastError());
   return APHID_OK;
+}
+
+int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx) {
+  if (!ctx) return APHID_ERR_BADARG;
+  return ctx->sw_work ? ctx->ptiles.kz : 0;
 }
 
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x) {

@@ -712,6 +712,79 @@ __device__ __forceinline__ float2 cfma(float2 a, float2 x, float2 y) {  // y + a
   return make_float2(fmaf(a.x, x.x, fmaf(-a.y, x.y, y.x)), fmaf(a.x, x.y, fmaf(a.y, x.x, y.y)));
 }
 
+
+// Stencil rows of the complex64 pass in difference form, with the sums as
+// trees (see k_sw_pass).  Edge row (Ax, Ay or Az): own value u0, six
+// neighbours n_k with real coefficients c_k, the Phi values f1 (ahead along
+// the edge) and f0, 1/d of the edge, vol; sigma-bar of the edge (s0), of
+// Phi ahead (spn) and at the node (sp0).  Model R: k^2 = (-ka, kb s).
+__device__ __forceinline__ float2 edge_row(float2 u0, float2 n1, float c1, float2 n2, float c2, float2 n3, float c3,
+                                           float2 n4, float c4, float2 n5, float c5, float2 n6, float c6, float s0,
+                                           float spn, float sp0, float2 f1, float2 f0, float rd, float vol, float ka,
+                                           float kb) {
+  const float2 t1 = axpy(c2, csub(n2, u0), rmul(c1, csub(n1, u0)));
+  const float2 t2 = axpy(c4, csub(n4, u0), rmul(c3, csub(n3, u0)));
+  const float2 t3 = axpy(c6, csub(n6, u0), rmul(c5, csub(n5, u0)));
+  const float2 L = cadd(cadd(t1, t2), axpy(-ka, u0, t3));
+  const float2 M = axpy(rd * (spn - sp0), f0, axpy(rd * (spn - s0), csub(f1, f0), rmul(s0, u0)));
+  return make_float2(vol * (L.x - kb * M.y), vol * (L.y + kb * M.x));
+}
+// the same with complex k^2 of the edge (k2), of Phi ahead (kpn) and at the
+// node (kp0): models C, I
+__device__ __forceinline__ float2 edge_row_c(float2 u0, float2 n1, float c1, float2 n2, float c2, float2 n3, float c3,
+                                             float2 n4, float c4, float2 n5, float c5, float2 n6, float c6, float2 k2,
+                                             float2 kpn, float2 kp0, float2 f1, float2 f0, float rd, float vol) {
+  const float2 t1 = axpy(c2, csub(n2, u0), rmul(c1, csub(n1, u0)));
+  const float2 t2 = axpy(c4, csub(n4, u0), rmul(c3, csub(n3, u0)));
+  const float2 t3 = axpy(c6, csub(n6, u0), rmul(c5, csub(n5, u0)));
+  const float2 g = cfma(make_float2(rd * (kpn.x - kp0.x), rd * (kpn.y - kp0.y)), f0,
+                        cfma(make_float2(rd * (kpn.x - k2.x), rd * (kpn.y - k2.y)), csub(f1, f0), cmul(k2, u0)));
+  const float2 L = cadd(cadd(t1, t2), cadd(t3, g));
+  return make_float2(vol * L.x, vol * L.y);
+}
+// Node row (Phi): own f, neighbours fx+ fx- fy+ fy- fz+ fz-, axis coefficients
+// n4/n5 per axis, the edges of the node (a0, a1, a2) and those behind it
+// (a0m, a1m, a2m), 1/dc per axis, sigma-bar of the six edges and of the node:
+// k_p^2 Phi + sum c_m (Phi_m - Phi) + sum_a [(k_a - k_p)(A_a - A_a-) +
+// (k_a - k_a-) A_a-] / dc_a with c_m = n_m k^2_m.  Model R.
+__device__ __forceinline__ float2 node_row(float2 f, float2 fxp, float2 fxm, float2 fyp, float2 fym, float2 fzp,
+                                           float2 fzm, float xn4, float xn5, float yn4, float yn5, float zn4,
+                                           float zn5, float2 a0, float2 a0m, float2 a1, float2 a1m, float2 a2,
+                                           float2 a2m, float rdxc, float rdyc, float rdzc, float sx, float sxm,
+                                           float sy, float sym, float sz, float szm, float sp0, float vol, float ka,
+                                           float kb) {
+  const float2 g1 = csub(fxp, f), g2 = csub(fxm, f), g3 = csub(fyp, f), g4 = csub(fym, f), g5 = csub(fzp, f),
+               g6 = csub(fzm, f);
+  const float2 T1 = cadd(cadd(axpy(xn5, g2, rmul(xn4, g1)), axpy(yn5, g4, rmul(yn4, g3))),
+                         axpy(zn5, g6, rmul(zn4, g5)));
+  const float2 T2a = cadd(axpy(xn5 * sxm, g2, rmul(xn4 * sx, g1)), axpy(yn5 * sym, g4, rmul(yn4 * sy, g3)));
+  const float2 T2b = axpy(zn5 * szm, g6, rmul(zn4 * sz, g5));
+  const float2 Ea = axpy(rdxc * (sx - sxm), a0m, rmul(rdxc * (sx - sp0), csub(a0, a0m)));
+  const float2 Eb = axpy(rdyc * (sy - sym), a1m, rmul(rdyc * (sy - sp0), csub(a1, a1m)));
+  const float2 Ec = axpy(rdzc * (sz - szm), a2m, rmul(rdzc * (sz - sp0), csub(a2, a2m)));
+  const float2 T2 = cadd(cadd(T2a, T2b), cadd(cadd(Ea, Eb), Ec));
+  const float2 t = cfma(make_float2(ka * ka - kb * kb * sp0 * sp0, -2.f * ka * kb * sp0), f,
+                        make_float2(-ka * T1.x, -ka * T1.y));
+  return make_float2(vol * (t.x - kb * T2.y), vol * (t.y + kb * T2.x));
+}
+// the same with complex k^2 (models C, I)
+__device__ __forceinline__ float2 node_row_c(float2 f, float2 fxp, float2 fxm, float2 fyp, float2 fym, float2 fzp,
+                                             float2 fzm, float xn4, float xn5, float yn4, float yn5, float zn4,
+                                             float zn5, float2 a0, float2 a0m, float2 a1, float2 a1m, float2 a2,
+                                             float2 a2m, float rdxc, float rdyc, float rdzc, float2 kx, float2 kxm,
+                                             float2 ky, float2 kym, float2 kz, float2 kzm, float2 kp, float vol) {
+  const float2 g1 = csub(fxp, f), g2 = csub(fxm, f), g3 = csub(fyp, f), g4 = csub(fym, f), g5 = csub(fzp, f),
+               g6 = csub(fzm, f);
+  const float2 Ta = cfma(rmul(xn5, kxm), g2, cmul(rmul(xn4, kx), g1));
+  const float2 Tb = cfma(rmul(yn5, kym), g4, cmul(rmul(yn4, ky), g3));
+  const float2 Tc = cfma(rmul(zn5, kzm), g6, cmul(rmul(zn4, kz), g5));
+  const float2 Ea = cfma(rmul(rdxc, csub(kx, kxm)), a0m, cmul(rmul(rdxc, csub(kx, kp)), csub(a0, a0m)));
+  const float2 Eb = cfma(rmul(rdyc, csub(ky, kym)), a1m, cmul(rmul(rdyc, csub(ky, kp)), csub(a1, a1m)));
+  const float2 Ec = cfma(rmul(rdzc, csub(kz, kzm)), a2m, cmul(rmul(rdzc, csub(kz, kp)), csub(a2, a2m)));
+  const float2 t = cadd(cadd(cadd(Ta, Tb), cadd(Tc, cmul(cmul(kp, kp), f))), cadd(cadd(Ea, Eb), Ec));
+  return make_float2(vol * t.x, vol * t.y);
+}
+
 // Scalar step at the end of pass n (one thread): epsilon_n, beta_n,
 // rho_{n+1} and delta_{n+1} from the pipelined inner products, then theta,
 // c, eta, kappa, tau and k1 as in src/aphid_qmr.f90:324-372.
@@ -1001,134 +1074,46 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
       const float zn4 = ZA.x, zn5 = ZA.y, dzc = ZA.z, rdzc = ZA.w, ce2z = ZB.x, ce3z = ZB.y, dzk = ZB.z,
                   rdzk = ZB.w;
       const float2 *U0 = Uc, *U1 = Uc + kPN, *U2 = Uc + 2 * kPN, *U3 = Uc + 3 * kPN;
-      float2 w[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-      // k^2 = (-ka e, kb s) of a component value
-      auto K2 = [&](float s_, float e_) { return make_float2(-ka * e_, kb * s_); };
-      auto dif = [](float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); };
-      if (hx) {
-        const float vol = dxi * dyc * dzc;
-        const float spx = rk[3 * kKN + ck + 1];
-        const float2 u0 = uc[0], f1 = U3[eo + 1], f0 = uc[3];
-        float2 L = make_float2(ce2x * (U0[eo + 1].x - u0.x), ce2x * (U0[eo + 1].y - u0.y));
-        L = axpy(ce3x, dif(U0[eo - 1], u0), L);
-        L = axpy(yn4, dif(U0[eo + kPW], u0), L);
-        L = axpy(yn5, dif(U0[eo - kPW], u0), L);
-        L = axpy(zn4, dif(up[0], u0), L);
-        L = axpy(zn5, dif(um[0], u0), L);
-        if (!EPS) {
-          L = axpy(-ka, u0, L);
-          float2 Mv = make_float2(sx * u0.x, sx * u0.y);
-          Mv = axpy(rdxi * (spx - sx), dif(f1, f0), Mv);
-          Mv = axpy(rdxi * (spx - sp0), f0, Mv);
-          w[0] = make_float2(vol * (L.x - kb * Mv.y), vol * (L.y + kb * Mv.x));
-        } else {
-          const float2 k2 = K2(sx, ex), kpx = K2(spx, re[3 * kKN + ck + 1]), kp0 = K2(sp0, ep0);
-          L = cfma(k2, u0, L);
-          L = cfma(make_float2(rdxi * (kpx.x - k2.x), rdxi * (kpx.y - k2.y)), dif(f1, f0), L);
-          L = cfma(make_float2(rdxi * (kpx.x - kp0.x), rdxi * (kpx.y - kp0.y)), f0, L);
-          w[0] = make_float2(vol * L.x, vol * L.y);
-        }
+      // Rows in difference form: k^2 u0 + sum c (u_nb - u0) for
+      // (-sum c + k^2) u0 + sum c u_nb, and (kp' - k^2)(Phi' - Phi) +
+      // (kp' - kp) Phi for Phi' (kp' - k^2) - Phi (kp - k^2): equal in exact
+      // arithmetic, and in FP32 free of the cancellation between the diagonal
+      // and the neighbours that a smooth field causes.  All four rows are
+      // formed without branches (boundary rows are zeroed after) and summed
+      // as trees, so that the rows interleave.
+      const float spx = rk[3 * kKN + ck + 1], spy = rk[3 * kKN + ck + kKW];
+      const float sxm = rk[ck - 1], sym = rk[kKN + ck - kKW];
+      const float2 f0 = uc[3];
+      float2 w0, w1, w2, w3;
+      if (!EPS) {
+        w0 = edge_row(uc[0], U0[eo + 1], ce2x, U0[eo - 1], ce3x, U0[eo + kPW], yn4, U0[eo - kPW], yn5, up[0], zn4,
+                      um[0], zn5, sx, spx, sp0, U3[eo + 1], f0, rdxi, dxi * dyc * dzc, ka, kb);
+        w1 = edge_row(uc[1], U1[eo + kPW], ce2y, U1[eo - kPW], ce3y, U1[eo + 1], xn4, U1[eo - 1], xn5, up[1], zn4,
+                      um[1], zn5, sy, spy, sp0, U3[eo + kPW], f0, rdyj, dxc * dyj * dzc, ka, kb);
+        w2 = edge_row(uc[2], up[2], ce2z, um[2], ce3z, U2[eo + 1], xn4, U2[eo - 1], xn5, U2[eo + kPW], yn4,
+                      U2[eo - kPW], yn5, sz, s3p, sp0, up[3], f0, rdzk, dxc * dyc * dzk, ka, kb);
+        w3 = node_row(f0, U3[eo + 1], U3[eo - 1], U3[eo + kPW], U3[eo - kPW], up[3], um[3], xn4, xn5, yn4, yn5, zn4,
+                      zn5, uc[0], U0[eo - 1], uc[1], U1[eo - kPW], uc[2], um[2], rdxc, rdyc, rdzc, sx, sxm, sy, sym,
+                      sz, s2m, sp0, dxc * dyc * dzc, ka, kb);
+      } else {
+        auto K2 = [&](float s_, float e_) { return make_float2(-ka * e_, kb * s_); };
+        const float2 kp0 = K2(sp0, ep0);
+        const float2 kx = K2(sx, ex), ky = K2(sy, ey), kz = K2(sz, ez);
+        w0 = edge_row_c(uc[0], U0[eo + 1], ce2x, U0[eo - 1], ce3x, U0[eo + kPW], yn4, U0[eo - kPW], yn5, up[0], zn4,
+                        um[0], zn5, kx, K2(spx, re[3 * kKN + ck + 1]), kp0, U3[eo + 1], f0, rdxi, dxi * dyc * dzc);
+        w1 = edge_row_c(uc[1], U1[eo + kPW], ce2y, U1[eo - kPW], ce3y, U1[eo + 1], xn4, U1[eo - 1], xn5, up[1], zn4,
+                        um[1], zn5, ky, K2(spy, re[3 * kKN + ck + kKW]), kp0, U3[eo + kPW], f0, rdyj,
+                        dxc * dyj * dzc);
+        w2 = edge_row_c(uc[2], up[2], ce2z, um[2], ce3z, U2[eo + 1], xn4, U2[eo - 1], xn5, U2[eo + kPW], yn4,
+                        U2[eo - kPW], yn5, kz, K2(s3p, e3p), kp0, up[3], f0, rdzk, dxc * dyc * dzk);
+        w3 = node_row_c(f0, U3[eo + 1], U3[eo - 1], U3[eo + kPW], U3[eo - kPW], up[3], um[3], xn4, xn5, yn4, yn5, zn4,
+                        zn5, uc[0], U0[eo - 1], uc[1], U1[eo - kPW], uc[2], um[2], rdxc, rdyc, rdzc, kx,
+                        K2(sxm, re[ck - 1]), ky, K2(sym, re[kKN + ck - kKW]), kz, K2(s2m, e2m), kp0,
+                        dxc * dyc * dzc);
       }
-      if (hy) {
-        const float vol = dxc * dyj * dzc;
-        const float spy = rk[3 * kKN + ck + kKW];
-        const float2 u0 = uc[1], f1 = U3[eo + kPW], f0 = uc[3];
-        float2 L = make_float2(ce2y * (U1[eo + kPW].x - u0.x), ce2y * (U1[eo + kPW].y - u0.y));
-        L = axpy(ce3y, dif(U1[eo - kPW], u0), L);
-        L = axpy(xn4, dif(U1[eo + 1], u0), L);
-        L = axpy(xn5, dif(U1[eo - 1], u0), L);
-        L = axpy(zn4, dif(up[1], u0), L);
-        L = axpy(zn5, dif(um[1], u0), L);
-        if (!EPS) {
-          L = axpy(-ka, u0, L);
-          float2 Mv = make_float2(sy * u0.x, sy * u0.y);
-          Mv = axpy(rdyj * (spy - sy), dif(f1, f0), Mv);
-          Mv = axpy(rdyj * (spy - sp0), f0, Mv);
-          w[1] = make_float2(vol * (L.x - kb * Mv.y), vol * (L.y + kb * Mv.x));
-        } else {
-          const float2 k2 = K2(sy, ey), kpy = K2(spy, re[3 * kKN + ck + kKW]), kp0 = K2(sp0, ep0);
-          L = cfma(k2, u0, L);
-          L = cfma(make_float2(rdyj * (kpy.x - k2.x), rdyj * (kpy.y - k2.y)), dif(f1, f0), L);
-          L = cfma(make_float2(rdyj * (kpy.x - kp0.x), rdyj * (kpy.y - kp0.y)), f0, L);
-          w[1] = make_float2(vol * L.x, vol * L.y);
-        }
-      }
-      if (m < nz - 1) {
-        const float vol = dxc * dyc * dzk;
-        const float2 u0 = uc[2], f1 = up[3], f0 = uc[3];
-        float2 L = make_float2(ce2z * (up[2].x - u0.x), ce2z * (up[2].y - u0.y));
-        L = axpy(ce3z, dif(um[2], u0), L);
-        L = axpy(xn4, dif(U2[eo + 1], u0), L);
-        L = axpy(xn5, dif(U2[eo - 1], u0), L);
-        L = axpy(yn4, dif(U2[eo + kPW], u0), L);
-        L = axpy(yn5, dif(U2[eo - kPW], u0), L);
-        if (!EPS) {
-          L = axpy(-ka, u0, L);
-          float2 Mv = make_float2(sz * u0.x, sz * u0.y);
-          Mv = axpy(rdzk * (s3p - sz), dif(f1, f0), Mv);
-          Mv = axpy(rdzk * (s3p - sp0), f0, Mv);
-          w[2] = make_float2(vol * (L.x - kb * Mv.y), vol * (L.y + kb * Mv.x));
-        } else {
-          const float2 k2 = K2(sz, ez), kpz = K2(s3p, e3p), kp0 = K2(sp0, ep0);
-          L = cfma(k2, u0, L);
-          L = cfma(make_float2(rdzk * (kpz.x - k2.x), rdzk * (kpz.y - k2.y)), dif(f1, f0), L);
-          L = cfma(make_float2(rdzk * (kpz.x - kp0.x), rdzk * (kpz.y - kp0.y)), f0, L);
-          w[2] = make_float2(vol * L.x, vol * L.y);
-        }
-      }
-      if (pxy && m > 0 && m < nz - 1) {
-        // s1^2 Phi + sum c_m (Phi_m - Phi) + sum_a [(k_a - s1)(A_a - A_a-) + (k_a - k_a-) A_a-] / dc_a
-        const float vol = dxc * dyc * dzc;
-        const float sxm = rk[ck - 1], sym = rk[kKN + ck - kKW];
-        const float2 f = uc[3];
-        const float2 g1 = dif(U3[eo + 1], f), g2 = dif(U3[eo - 1], f), g3 = dif(U3[eo + kPW], f);
-        const float2 g4 = dif(U3[eo - kPW], f), g5 = dif(up[3], f), g6 = dif(um[3], f);
-        const float2 a0m = U0[eo - 1], a1m = U1[eo - kPW], a2m = um[2];
-        const float2 h0 = dif(uc[0], a0m), h1 = dif(uc[1], a1m), h2 = dif(uc[2], a2m);
-        if (!EPS) {
-          float2 T1 = make_float2(xn4 * g1.x, xn4 * g1.y);
-          T1 = axpy(xn5, g2, T1);
-          T1 = axpy(yn4, g3, T1);
-          T1 = axpy(yn5, g4, T1);
-          T1 = axpy(zn4, g5, T1);
-          T1 = axpy(zn5, g6, T1);
-          float2 T2 = make_float2(xn4 * sx * g1.x, xn4 * sx * g1.y);
-          T2 = axpy(xn5 * sxm, g2, T2);
-          T2 = axpy(yn4 * sy, g3, T2);
-          T2 = axpy(yn5 * sym, g4, T2);
-          T2 = axpy(zn4 * sz, g5, T2);
-          T2 = axpy(zn5 * s2m, g6, T2);
-          T2 = axpy(rdxc * (sx - sp0), h0, T2);
-          T2 = axpy(rdxc * (sx - sxm), a0m, T2);
-          T2 = axpy(rdyc * (sy - sp0), h1, T2);
-          T2 = axpy(rdyc * (sy - sym), a1m, T2);
-          T2 = axpy(rdzc * (sz - sp0), h2, T2);
-          T2 = axpy(rdzc * (sz - s2m), a2m, T2);
-          const float2 t = cfma(make_float2(ka * ka - kb * kb * sp0 * sp0, -2.f * ka * kb * sp0), f,
-                                make_float2(-ka * T1.x, -ka * T1.y));
-          w[3] = make_float2(vol * (t.x - kb * T2.y), vol * (t.y + kb * T2.x));
-        } else {
-          const float exm = re[ck - 1], eym = re[kKN + ck - kKW];
-          const float2 s1 = K2(sp0, ep0);
-          const float2 s2 = K2(sx, ex), s3 = K2(sxm, exm), s4 = K2(sy, ey), s5 = K2(sym, eym);
-          const float2 s6 = K2(sz, ez), s7 = K2(s2m, e2m);
-          const float2 s11 = cmul(s1, s1);
-          float2 t = cfma(s11, f, make_float2(0.f, 0.f));
-          t = cfma(make_float2(xn4 * s2.x, xn4 * s2.y), g1, t);
-          t = cfma(make_float2(xn5 * s3.x, xn5 * s3.y), g2, t);
-          t = cfma(make_float2(yn4 * s4.x, yn4 * s4.y), g3, t);
-          t = cfma(make_float2(yn5 * s5.x, yn5 * s5.y), g4, t);
-          t = cfma(make_float2(zn4 * s6.x, zn4 * s6.y), g5, t);
-          t = cfma(make_float2(zn5 * s7.x, zn5 * s7.y), g6, t);
-          t = cfma(make_float2(rdxc * (s2.x - s1.x), rdxc * (s2.y - s1.y)), h0, t);
-          t = cfma(make_float2(rdxc * (s2.x - s3.x), rdxc * (s2.y - s3.y)), a0m, t);
-          t = cfma(make_float2(rdyc * (s4.x - s1.x), rdyc * (s4.y - s1.y)), h1, t);
-          t = cfma(make_float2(rdyc * (s4.x - s5.x), rdyc * (s4.y - s5.y)), a1m, t);
-          t = cfma(make_float2(rdzc * (s6.x - s1.x), rdzc * (s6.y - s1.y)), h2, t);
-          t = cfma(make_float2(rdzc * (s6.x - s7.x), rdzc * (s6.y - s7.y)), a2m, t);
-          w[3] = make_float2(vol * t.x, vol * t.y);
-        }
-      }
+      const float2 zero2 = make_float2(0.f, 0.f);
+      float2 w[4] = {hx ? w0 : zero2, hy ? w1 : zero2, m < nz - 1 ? w2 : zero2,
+                     (pxy && m > 0 && m < nz - 1) ? w3 : zero2};
       // the Jacobi diagonal of this node (the same function the residual
       // pass uses, on the same values)
       float2 dg[4];

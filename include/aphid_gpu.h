@@ -66,8 +66,10 @@ typedef struct {
   void *stream;      /* cudaStream_t to run on; NULL = a stream owned by the context */
   int graph_iters;   /* QMR iterations per CUDA-graph launch; 0 = default (16) */
   int verbose;       /* 1 = progress lines on stderr */
-  int plane_kz;      /* z-planes per block of the complex64 operator pass;
-                        0 = chosen from the mesh (the autotuner sets it) */
+  int plane_kz;      /* z-planes per work item of the complex64 pass (>= 4);
+                        0 = autotuned: timed on the device for each new
+                        (mesh, batch, model kind) and cached, in the process
+                        and in the file named by APHID_TUNE_CACHE if set */
 } aphid_opts;
 
 typedef struct {
@@ -220,6 +222,11 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega,
                     const char *dip_dir, const int *dip_ijk, const aphid_z *x0,
                     const aphid_sweep_opts *opts, aphid_z *x_out,
                     aphid_info *info);
+
+/* z-planes per work item of the complex64 pass in use (the autotuner's
+ * choice unless aphid_opts.plane_kz fixed it); 0 before the first mixed
+ * sweep. */
+int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx);
 
 /* Copy system `sys` of the last sweep into x (one [x|y|z|p] vector). */
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);

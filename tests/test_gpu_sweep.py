@@ -165,3 +165,33 @@ def test_sweep_rejects_bad_input(solver):
     solver.set_model("R", sig)
     with pytest.raises(AphidError):
         solver.sweep([1.0], [[("+X", 6, 6, 4)]], [3])
+
+
+def test_autotuner_picks_and_caches_the_slab_depth(tmp_path, monkeypatch):
+    """plane_kz = 0: the pass depth is timed on the device per (mesh, batch,
+    model kind), kept in the process and in APHID_TUNE_CACHE; a fixed
+    plane_kz overrides it.  The solution does not depend on the choice."""
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("APHID_TUNE_CACHE", str(cache))
+    xn, yn, zn, sig, _ = small_model(seed=11, dims=(18, 17, 26))
+    src = [[("+X", 8, 8, 4)]]
+    w = [2 * np.pi * f for f in (0.5, 50.0)]
+    with Solver(graph_iters=8) as s:
+        s.set_nodes(xn, yn, zn)
+        s.set_model("R", sig)
+        X1, i1 = s.sweep(w, src, [0, 0])
+        kz = s.sweep_plane_kz()
+        assert kz in (4, 6, 8, 12, 16, 24, 32) and kz <= len(zn)
+        X2, _ = s.sweep(w, src, [0, 0])
+        assert s.sweep_plane_kz() == kz          # cached, not retuned
+        assert np.array_equal(X1, X2)            # same depth, same bits
+    lines = cache.read_text().split()
+    assert lines[-6:] == [str(v) for v in (18, 17, 26, 2, 0, kz)]
+    with Solver(graph_iters=8, plane_kz=8) as s:
+        s.set_nodes(xn, yn, zn)
+        s.set_model("R", sig)
+        X3, i3 = s.sweep(w, src, [0, 0])
+        assert s.sweep_plane_kz() == 8
+    for a, b, ia, ib in zip(X1, X3, i1, i3):
+        assert ia["status_name"] == ib["status_name"] == "converged"
+        assert relerr(a, b) < 1e-6
