@@ -24,14 +24,15 @@ def up_to_date():
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    hdr = os.path.join(os.path.dirname(HERE), "include", "aphid_gpu.h")
-    return all(os.path.getmtime(s) <= t for s in sources() + [hdr])
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    hdrs = [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
+    return all(os.path.getmtime(s) <= t for s in sources() + hdrs)
 
 
 def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
-    units = [os.path.join(SRC, f) for f in ("aphid_gpu.cu", "aphid_noalloc.cu")]
+    units = [os.path.join(SRC, f) for f in ("aphid_gpu.cu", "aphid_noalloc.cu", "aphid_unet.cu")]
     cmd = ["nvcc"] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB] + units
     subprocess.run(cmd, check=True)
     return LIB

@@ -229,6 +229,8 @@ def main():
                     help="timed complex128 solves for the speed-up comparison (0: skip)")
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--one-sweep", action="store_true",
+                    help="run one mixed sweep of the workload and exit (profiling target)")
     ap.add_argument("--only-apply", action="store_true",
                     help="set up the workload and time only the operator apply (profiling)")
     args = ap.parse_args()
@@ -267,6 +269,16 @@ def main():
     nsys = len(om)
     peak, peak_kind = peaks()
     clocks = ClockSampler(local)
+
+    if args.one_sweep:
+        # one mixed sweep of the workload, nothing timed (profiling target)
+        s.set_model("R", m.sig_re)
+        _, inf = s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=MAX_IT, fetch=False)
+        print(json.dumps({"workload": args.workload, "systems": nsys, "plane_kz": s.sweep_plane_kz(),
+                          "inner_iters": [i["inner_iters"] for i in inf][:8],
+                          "outer_iters": [i["outer_iters"] for i in inf][:8],
+                          "seconds": inf[0]["seconds"], "launches": inf[0]["kernel_launches"]}))
+        return 0
 
     if args.only_apply and args.precision == "mixed":
         # resident complex64 state from a short sweep, then the operator pass

@@ -20,7 +20,7 @@ def declared_functions():
         if h.endswith(".h"):
             txt = open(os.path.join(ROOT, "include", h)).read()
             txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-            names += re.findall(r"\b(aphid_gpu_\w+)\s*\(", txt)
+            names += re.findall(r"\b(aphid_(?:gpu|unet)_\w+)\s*\(", txt)
     return sorted(set(names))
 
 
