@@ -178,6 +178,7 @@ class Solver:
         from .model import spacings
         (dx, dxc), (dy, dyc), (dz, dzc) = spacings(xn), spacings(yn), spacings(zn)
         self.set_mesh(dx, dy, dz, dxc, dyc, dzc)
+        self.xn, self.yn, self.zn = (np.asarray(v, np.float64) for v in (xn, yn, zn))
 
     def _blocks(self, v):
         b = v.ctypes.data

@@ -36,6 +36,39 @@ const char *aphid_unet_last_error(void);
 int aphid_unet_gemm_bf16(const void *A, int lda, const void *B, int ldb, void *C, int ldc, const float *bias,
                          int M, int N, int K, int out, int splitk, void *stream, int *err_flag);
 
+/* ---- the network --------------------------------------------------------
+ * 3-D U-Net: four levels of 16/32/64/128 channels, two 3x3x3 convolutions
+ * with ReLU per level and side, 2x2x2 mean pooling, nearest upsampling with
+ * skip concatenation, a 3x3x3 head to 8 channels.  Weights BF16 on the
+ * tensor cores with FP32 master copies (Adam); activations BF16; FP32
+ * accumulation.  A network object holds the buffers for one volume of
+ * nodes (X, Y, Z), internally padded to multiples of 8; parameters move
+ * between objects of different volumes through get/set_params.
+ * Parameter layout (host, FP32): per layer W[co][tap*cin + ci], then b[co],
+ * tap = ((dz+1)*3 + (dy+1))*3 + (dx+1), layers in the order
+ * 3-16, 16-16, 16-32, 32-32, 32-64, 64-64, 64-128, 128-128, 192-64, 64-64,
+ * 96-32, 32-32, 48-16, 16-16, 16-8.
+ * Features x: [V][3] and targets / outputs [V][8] (FP32, device), voxel
+ * v = i + X (j + Y k). */
+typedef struct aphid_unet aphid_unet;
+
+long long aphid_unet_param_count(void);
+/* train = 0: inference buffers only.  seed: the initial He-normal weights. */
+int aphid_unet_create(aphid_unet **net, int X, int Y, int Z, int train, unsigned long long seed);
+int aphid_unet_destroy(aphid_unet *net);
+int aphid_unet_get_params(aphid_unet *net, float *host);
+int aphid_unet_set_params(aphid_unet *net, const float *host);  /* also resets the optimiser */
+/* y = net(x); synchronises the stream. */
+int aphid_unet_forward(aphid_unet *net, const float *x, float *y, void *stream);
+/* One step on (x, target): loss = sum_v w_v sum_c (y - t)^2 / (8 sum_v w_v)
+ * (weight NULL: all ones), its gradient by back-propagation, and, when
+ * update != 0, one Adam step (lr; betas 0.9, 0.999).  Synchronises the
+ * stream; *loss is the loss before the update. */
+int aphid_unet_train_step(aphid_unet *net, const float *x, const float *target, const float *weight, float lr,
+                          int update, double *loss, void *stream);
+/* The parameter gradient of the last train step, in the parameter layout. */
+int aphid_unet_get_grads(aphid_unet *net, float *host);
+
 #ifdef __cplusplus
 }
 #endif
