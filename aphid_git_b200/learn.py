@@ -259,6 +259,49 @@ def evaluate(params, seeds, freqs, config="eval160", max_it=20000, verbose=True)
     return rows
 
 
+def conv_flops(dims):
+    """FLOPs of one forward pass (the GEMMs of the 15 convolutions)"""
+    from . import unet  # noqa: F401  (same layer list as the device code)
+    layers = [(3, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 128, 3),
+              (128, 128, 3), (192, 64, 2), (64, 64, 2), (96, 32, 1), (32, 32, 1), (48, 16, 0), (16, 16, 0),
+              (16, 8, 0)]
+    v0 = np.prod([-(-d // 8) * 8 for d in dims])
+    return sum(2.0 * v0 / 8 ** lev * 27 * ci * co for ci, co, lev in layers)
+
+
+def speed(dims, steps):
+    """ms per training step and per forward pass, and the GEMM FLOP rate
+    (backward = twice the forward FLOPs: dW and dCol)"""
+    import torch
+    from . import unet
+    rng = np.random.default_rng(0)
+    V = int(np.prod(dims))
+    x = torch.from_numpy(rng.standard_normal((V, 3)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((V, 8)).astype(np.float32) * 0.1).cuda()
+    y = torch.empty(V, 8, device="cuda")
+    out = {"dims": list(dims), "forward_gflop": conv_flops(dims) / 1e9}
+    with unet.UNet(*dims, train=True) as net:
+        for _ in range(3):
+            net.train_step(x, t, lr=1e-4)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        for _ in range(steps):
+            net.train_step(x, t, lr=1e-4)
+        torch.cuda.synchronize()
+        out["train_step_ms"] = (time.time() - t0) / steps * 1e3
+        for _ in range(3):
+            net.forward(x, y)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        for _ in range(steps):
+            net.forward(x, y)
+        torch.cuda.synchronize()
+        out["forward_ms"] = (time.time() - t0) / steps * 1e3
+    out["train_tflops"] = 3 * out["forward_gflop"] / out["train_step_ms"]
+    out["forward_tflops"] = out["forward_gflop"] / out["forward_ms"]
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -274,7 +317,13 @@ def main(argv=None):
     e.add_argument("--config", default="eval160")
     e.add_argument("--seeds", type=int, nargs="+", default=[901, 902])
     e.add_argument("--freqs", type=float, nargs="+", default=[1e-2, 1.0, 1e2])
+    sp = sub.add_parser("speed")
+    sp.add_argument("--dims", type=int, nargs=3, default=[65, 65, 49])
+    sp.add_argument("--steps", type=int, default=20)
     a = ap.parse_args(argv)
+    if a.cmd == "speed":
+        print(json.dumps(speed(tuple(a.dims), a.steps)))
+        return
     if a.cmd == "train":
         rng = np.random.default_rng(a.first_seed)
         t0 = time.time()
