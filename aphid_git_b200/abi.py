@@ -19,7 +19,8 @@ APHID_OK = 0
 STATUS = {0: "converged", 1: "maxit", 2: "breakdown", 3: "nonfinite"}
 ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "out of device memory",
           -4: "call order", -5: "no sm_100 device"}
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FUSED64, PREC_AUTO = 0, 1, 2, 3
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED, "fused64": PREC_FUSED64, "auto": PREC_AUTO}
 
 
 class AphidError(RuntimeError):
@@ -28,7 +29,8 @@ class AphidError(RuntimeError):
 
 class SweepOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("target", C.c_double), ("max_it", C.c_int),
-                ("inner_tol", C.c_double), ("max_outer", C.c_int), ("reserved", C.c_int * 3)]
+                ("inner_tol", C.c_double), ("max_outer", C.c_int), ("stall_window", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 class Opts(C.Structure):
@@ -40,7 +42,7 @@ class Info(C.Structure):
     _fields_ = [("status", C.c_int), ("iters", C.c_int), ("inner_iters", C.c_int),
                 ("outer_iters", C.c_int), ("rhs_norm", C.c_double), ("recur_resid", C.c_double),
                 ("true_rel_resid", C.c_double), ("seconds", C.c_double),
-                ("kernel_launches", C.c_longlong)]
+                ("kernel_launches", C.c_longlong), ("inner64_iters", C.c_int)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_}
@@ -87,6 +89,7 @@ def load():
                                   C.POINTER(SweepOpts), P, P]
     L.aphid_gpu_sweep_fetch.argtypes = [P, C.c_int, P]
     L.aphid_gpu_sweep_time_apply.argtypes = [P, C.c_int]
+    L.aphid_gpu_sweep_apply.argtypes = [P, _Z, _Z]
     L.aphid_gpu_sweep_plane_kz.argtypes = [P]
     _lib = L
     return L
@@ -278,7 +281,7 @@ class Solver:
             self._model[1].ctypes.data if self._model[1] is not None else None), "set_model")
 
     def sweep(self, omegas, sources, source_of_system=None, x0=None, precision="mixed",
-              target=1e-8, max_it=20000, inner_tol=0.0, max_outer=0, fetch=True):
+              target=1e-8, max_it=20000, inner_tol=0.0, max_outer=0, stall_window=0, fetch=True):
         """Solve all (omega, source) systems in one batched launch.
 
         sources: list of oper_mode-5 dipole lists [(dir, i, j, k), ...];
@@ -296,8 +299,10 @@ class Solver:
         x0a = None if x0 is None else np.ascontiguousarray(x0, dtype=np.complex128).reshape(nsys, self.n)
         X = np.empty((nsys, self.n), np.complex128) if fetch else None
         infos = (Info * nsys)()
-        o = SweepOpts(PREC_MIXED if precision == "mixed" else PREC_FP64, float(target), int(max_it),
-                      float(inner_tol), int(max_outer))
+        if precision not in PRECISIONS:
+            raise AphidError("precision must be one of %s" % ", ".join(PRECISIONS))
+        o = SweepOpts(PRECISIONS[precision], float(target), int(max_it),
+                      float(inner_tol), int(max_outer), int(stall_window))
         self._check(self.lib.aphid_gpu_sweep(
             self._h, nsys, om.ctypes.data, sos.ctypes.data, len(sources), ndip.ctypes.data,
             dirs or b"  ", ijk.ctypes.data, x0a.ctypes.data if x0a is not None else None,
@@ -309,6 +314,15 @@ class Solver:
         systems of the last mixed sweep (asynchronous; for timing; the
         solutions are not changed)."""
         self._check(self.lib.aphid_gpu_sweep_time_apply(self._h, int(reps)), "sweep_time_apply")
+
+    def sweep_apply(self, x):
+        """y = K x through the fused pass of the last batched sweep (complex64
+        after mixed/auto, complex128 after fused64), for its system 0
+        (testing hook: overwrites that sweep's inner vectors)."""
+        x = np.ascontiguousarray(x, dtype=np.complex128).reshape(self.n)
+        y = np.empty(self.n, np.complex128)
+        self._check(self.lib.aphid_gpu_sweep_apply(self._h, x.ctypes.data, y.ctypes.data), "sweep_apply")
+        return y
 
     def sweep_plane_kz(self):
         """z-planes per work item of the complex64 pass in use (the

@@ -154,6 +154,7 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 rmul(float r, float2 b) { return make_float2(r * b.x, r * b.y); }
 __device__ __forceinline__ float2 rdiv(float2 a, float r) { return make_float2(a.x / r, a.y / r); }
 __device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ double2 to_d(double2 a) { return a; }
 __device__ __forceinline__ float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
 
 template <typename R> struct CplxOf;

@@ -12,6 +12,7 @@
 #include <mutex>
 #include <cmath>
 #include <cstdio>
+#include <climits>
 #include <cstring>
 #include <map>
 #include <string>
@@ -67,12 +68,16 @@ struct aphid_ctx {
   char csig = 'R';
   double *d_sig = nullptr, *d_epsr = nullptr;
   float *d_sig32 = nullptr, *d_epsr32 = nullptr;
+  double *d_sig64 = nullptr, *d_epsr64 = nullptr;  // FP64 node-layout copies (complex128 pass)
   // sweep state
   int sw_nsys = 0;           // systems the buffers hold
   bool sw_f32_ok = false;    // complex64 vectors allocated
   double2 *sw_f64 = nullptr; // [2][nsys][n]: x64, b
   float2 *sw_f32 = nullptr;  // [8][nsys][4][N]: 2 sets of q^ v^ p^, then d^ x^ (node layout)
   float4 *sw_ax32 = nullptr; // FP32 axis tables of the complex64 pass
+  double2 *sw_w64 = nullptr; // [8][nsys64][4][N]: the complex128 pass's q^ v^ p^ (2 sets), d^, x^
+  int sw_nsys64 = 0;         // systems sw_w64 holds
+  double4 *sw_ax64 = nullptr; // FP64 axis tables of the complex128 pass
   int *sw_work = nullptr;    // [2] work counter of the persistent pass, then [order]
   int num_sms = 148;         // multiprocessors of the device
   PassMaps maps{};           // TMA tensor maps of the pass
@@ -85,6 +90,7 @@ struct aphid_ctx {
   long long sw_slots = 0;
   int sw_bps = 0;
   int sw_last = 0;           // systems in the last sweep
+  bool sw_last_fused = false; // its inner storage was complex128 (FUSED64)
   cudaGraphExec_t sw_gexec = nullptr;
   int sw_gkey = 0;
 };
@@ -145,6 +151,11 @@ void release_work(aphid_ctx *ctx) {
   cudaFree(ctx->sw_f32);
   cudaFree(ctx->sw_ax32);
   ctx->sw_ax32 = nullptr;
+  cudaFree(ctx->sw_w64);
+  ctx->sw_w64 = nullptr;
+  ctx->sw_nsys64 = 0;
+  cudaFree(ctx->sw_ax64);
+  ctx->sw_ax64 = nullptr;
   cudaFree(ctx->sw_work);
   ctx->sw_work = nullptr;
   cudaFree(ctx->sw_sys);
@@ -309,6 +320,8 @@ int aphid_gpu_destroy(aphid_ctx *ctx) {
   cudaFree(ctx->d_epsr);
   cudaFree(ctx->d_sig32);
   cudaFree(ctx->d_epsr32);
+  cudaFree(ctx->d_sig64);
+  cudaFree(ctx->d_epsr64);
   if (ctx->h_done) cudaFreeHost(ctx->h_done);
   if (ctx->h_ndone) cudaFreeHost(ctx->h_ndone);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -343,11 +356,15 @@ int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz, const double *dx,
   cudaFree(ctx->d_epsr);
   cudaFree(ctx->d_sig32);
   cudaFree(ctx->d_epsr32);
+  cudaFree(ctx->d_sig64);
+  cudaFree(ctx->d_epsr64);
   ctx->d_tab = nullptr;
   ctx->d_sig = nullptr;
   ctx->d_epsr = nullptr;
   ctx->d_sig32 = nullptr;
   ctx->d_epsr32 = nullptr;
+  ctx->d_sig64 = nullptr;
+  ctx->d_epsr64 = nullptr;
   ctx->has_mesh = false;
   ctx->has_model = false;
 
@@ -735,6 +752,19 @@ int vector_maps(aphid_ctx *ctx) {
                     obox);
 }
 
+// complex128 q^, v^, p^ of both sets: 5-D (real/imaginary doubles along i,
+// j, k, vector x component, set x system) over 8-byte elements; one box = the
+// same 20 x 18 nodes of one z-plane as the complex64 map
+int vector_maps64(aphid_ctx *ctx) {
+  const NodeLayout &L = ctx->nl;
+  const cuuint64_t dims[5] = {2 * (cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 12,
+                              2 * (cuuint64_t)ctx->sw_nsys64};
+  const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * 16, (cuuint64_t)L.nxp * ctx->ny * 16, (cuuint64_t)L.N * 16,
+                                 (cuuint64_t)L.N * 192};
+  const cuuint32_t box[5] = {2 * kPW, kPH, 1, 12, 1};
+  return encode_map(ctx, &ctx->maps.w64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64, dims, strides, box);
+}
+
 // sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18
 int model_maps(aphid_ctx *ctx) {
   const NodeLayout &L = ctx->nl;
@@ -775,6 +805,15 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
     D.xx = ctx->sw_f32 + 7 * v32;
     D.ax32 = ctx->sw_ax32;
   }
+  if (ctx->sw_w64) {
+    const size_t v64 = (size_t)ctx->sw_nsys64 * 4 * ctx->nl.N;
+    D.W64 = ctx->sw_w64;
+    D.dd64 = ctx->sw_w64 + 6 * v64;
+    D.xx64 = ctx->sw_w64 + 7 * v64;
+    D.ax64 = ctx->sw_ax64;
+  }
+  D.sig64 = ctx->d_sig64;
+  D.epsr64 = ctx->d_epsr64;
   D.x64 = ctx->sw_f64;
   D.b = ctx->sw_f64 + vec;
   D.sys = ctx->sw_sys;
@@ -889,6 +928,32 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
   return APHID_OK;
 }
 
+// complex128 inner buffers of the fused FP64 pass for k systems
+int sweep_alloc64(aphid_ctx *ctx, int k) {
+  if (ctx->sw_w64 && k <= ctx->sw_nsys64) return APHID_OK;
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  cudaFree(ctx->sw_w64);
+  ctx->sw_w64 = nullptr;
+  ctx->sw_nsys64 = 0;
+  const size_t v64 = (size_t)k * 4 * ctx->nl.N;
+  if (cudaMalloc(&ctx->sw_w64, 8 * v64 * sizeof(double2)) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->sw_w64 = nullptr;
+    return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex128 inner vectors failed");
+  }
+  CK(cudaMemsetAsync(ctx->sw_w64, 0, 8 * v64 * sizeof(double2), ctx->stream));
+  if (!ctx->sw_ax64) {
+    CK(cudaMalloc(&ctx->sw_ax64, 2 * (size_t)(ctx->nx + ctx->ny + ctx->nz) * sizeof(double4)));
+    const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));
+    k_sw_axis64<<<dim3((unsigned)((nmax + 127) / 128), 3), 128, 0, ctx->stream>>>(ctx->g, ctx->sw_ax64);
+    CK(cudaGetLastError());
+  }
+  if (!ctx->sw_err) CK(cudaMalloc(&ctx->sw_err, sizeof(int)));
+  ctx->sw_nsys64 = k;
+  return vector_maps64(ctx);
+}
+
 // oper_mode 5 sources (src/aphid.f90:638-741) as sparse (index, value) lists
 // per source, duplicates accumulated in file order.
 void source_entries(const aphid_ctx *ctx, int nsrc, const int *src_ndip, const char *dir, const int *ijk,
@@ -939,6 +1004,11 @@ int pass_attrs(aphid_ctx *ctx) {
   CK(cudaFuncSetAttribute(k_sw_pass<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, r));
   CK(cudaFuncSetAttribute(k_sw_pass<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
   CK(cudaFuncSetAttribute(k_sw_pass<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
+  const int f = (int)kPass64Shm;
+  CK(cudaFuncSetAttribute(k_sw_pass64<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
+  CK(cudaFuncSetAttribute(k_sw_pass64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
+  CK(cudaFuncSetAttribute(k_sw_pass64<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
+  CK(cudaFuncSetAttribute(k_sw_pass64<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
   return APHID_OK;
 }
 
@@ -960,29 +1030,56 @@ void launch_pass(aphid_ctx *ctx, const SweepDev &D, bool timing) {
   }
 }
 
-void sweep_round(aphid_ctx *ctx, const SweepDev &D) {
-  const unsigned ps = (unsigned)(D.bps * D.nsys);
-  const unsigned st = (unsigned)(D.t.count() * D.nsys);
-  k_sw_xupd<<<ps, kStreamThreads, 0, ctx->stream>>>(D);
-  k_sw_resid<<<st, kOpThreads, 0, ctx->stream>>>(D);
-  for (int it = 0; it < ctx->graph_iters; it++) launch_pass(ctx, D, false);
-  k_sw_check<<<st, kOpThreads, 0, ctx->stream>>>(D);
+// the complex128 pass, persistent like launch_pass
+void launch_pass64(aphid_ctx *ctx, const SweepDev &D, bool timing) {
+  const long long items = D.tp.count() * D.nsys;
+  const unsigned sp = (unsigned)std::min<long long>(items, (long long)ctx->num_sms);
+  if (D.epsr64) {
+    if (timing)
+      k_sw_pass64<true, true><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
+    else
+      k_sw_pass64<true, false><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
+  } else {
+    if (timing)
+      k_sw_pass64<false, true><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
+    else
+      k_sw_pass64<false, false><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
+  }
 }
 
-int sweep_graph(aphid_ctx *ctx, const SweepDev &D) {
-  if (ctx->sw_gexec && ctx->sw_gkey == D.nsys) return APHID_OK;
+template <typename T>
+void sweep_round_t(aphid_ctx *ctx, const SweepDev &D) {
+  const unsigned ps = (unsigned)(D.bps * D.nsys);
+  const unsigned st = (unsigned)(D.t.count() * D.nsys);
+  k_sw_xupd<T><<<ps, kStreamThreads, 0, ctx->stream>>>(D);
+  k_sw_resid<T><<<st, kOpThreads, 0, ctx->stream>>>(D);
+  for (int it = 0; it < ctx->graph_iters; it++) {
+    if (sizeof(T) == sizeof(double2))
+      launch_pass64(ctx, D, false);
+    else
+      launch_pass(ctx, D, false);
+  }
+  k_sw_check<T><<<st, kOpThreads, 0, ctx->stream>>>(D);
+}
+
+int sweep_graph(aphid_ctx *ctx, const SweepDev &D, bool fused64) {
+  const int key = 2 * D.nsys + (fused64 ? 1 : 0);
+  if (ctx->sw_gexec && ctx->sw_gkey == key) return APHID_OK;
   int rc = pass_attrs(ctx);
   if (rc) return rc;
   if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
   ctx->sw_gexec = nullptr;
   cudaGraph_t graph;
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  sweep_round(ctx, D);
+  if (fused64)
+    sweep_round_t<double2>(ctx, D);
+  else
+    sweep_round_t<float2>(ctx, D);
   CK(cudaStreamEndCapture(ctx->stream, &graph));
   cudaError_t e = cudaGraphInstantiate(&ctx->sw_gexec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate (sweep)");
-  ctx->sw_gkey = D.nsys;
+  ctx->sw_gkey = key;
   return APHID_OK;
 }
 
@@ -1081,6 +1178,190 @@ int tune_kz(aphid_ctx *ctx, int nsys) {
   return APHID_OK;
 }
 
+// per-system state of a batched sweep at its start
+SweepSys sweep_sys_init(double omega, const aphid_sweep_opts *opts, bool fused, bool escalate, int max_it) {
+  SweepSys S{};
+  S.omega = omega;
+  S.ka = omega * omega * kMu0 * kEps0;
+  S.kb = omega * kMu0;
+  S.target = opts->target;
+  S.max_it = max_it;
+  S.inner_tol = opts->inner_tol > 0 ? opts->inner_tol : 1e-10;
+  S.max_outer = opts->max_outer > 0 ? opts->max_outer : 40;
+  // complex128 cycles do not stall the way complex64 ones do: no window
+  // unless asked for
+  S.stall_window = opts->stall_window > 0 ? opts->stall_window
+                   : (opts->stall_window < 0 || fused) ? INT_MAX : kStallWindow;
+  S.escalate = escalate ? 1 : 0;
+  S.phase = PH_OUTER;
+  S.status = -1;
+  return S;
+}
+
+aphid_info sweep_info(const SweepSys &S, bool fused) {
+  aphid_info I{};
+  I.status = S.status;
+  I.iters = S.total_it;
+  I.inner_iters = S.total_it;
+  I.inner64_iters = fused ? S.total_it : 0;
+  I.outer_iters = S.outer_it;
+  I.rhs_norm = S.bnorm;
+  I.recur_resid = S.tau;
+  I.true_rel_resid = S.bnorm > 0 ? S.rnorm / S.bnorm : S.rnorm;
+  return I;
+}
+
+// Graph rounds over the systems of D (x64 and b in place, SweepSys in hs)
+// until every system is done; hs is read back.
+int run_batched(aphid_ctx *ctx, const SweepDev &D, bool fused, std::vector<SweepSys> &hs, int max_it,
+                long long &nlaunch) {
+  const int nsys = D.nsys;
+  int rc;
+  CK(cudaMemcpyAsync(ctx->sw_sys, hs.data(), nsys * sizeof(SweepSys), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->sw_ndone, 0, sizeof(int), ctx->stream));
+  CK(cudaMemsetAsync(ctx->sw_err, 0, sizeof(int), ctx->stream));
+  k_sw_bnorm<<<(unsigned)(D.bps * nsys), kStreamThreads, 0, ctx->stream>>>(D);
+  CK(cudaGetLastError());
+  nlaunch += 1;
+  if ((rc = sweep_graph(ctx, D, fused))) return rc;
+  const long long per_round = 3 + (long long)ctx->graph_iters;
+  const long long max_rounds = (long long)std::max(1, max_it) / ctx->graph_iters + 2LL * (hs[0].max_outer + 2);
+  for (long long round = 0;; round++) {
+    CK(cudaMemcpyAsync(ctx->h_ndone, ctx->sw_ndone, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->h_ndone >= nsys) break;
+    if (round > max_rounds) return fail(ctx, APHID_ERR_STATE, "sweep did not terminate");
+    CK(cudaGraphLaunch(ctx->sw_gexec, ctx->stream));
+    nlaunch += per_round;
+  }
+  CK(cudaMemcpyAsync(hs.data(), ctx->sw_sys, nsys * sizeof(SweepSys), cudaMemcpyDeviceToHost, ctx->stream));
+  int kerr = 0;
+  CK(cudaMemcpyAsync(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (kerr) return fail(ctx, APHID_ERR_CUDA, "sweep: a tensor-copy wait in the operator pass timed out");
+  return APHID_OK;
+}
+
+// exchange the x and b slots of systems p and q (tmp: 2 n complex128)
+int swap_systems(aphid_ctx *ctx, int p, int q, double2 *tmp) {
+  if (p == q) return APHID_OK;
+  const size_t n = (size_t)ctx->n, bytes = n * sizeof(double2), cap = (size_t)ctx->sw_nsys * n;
+  double2 *base[2] = {ctx->sw_f64, ctx->sw_f64 + cap};
+  for (int v = 0; v < 2; v++) {
+    double2 *a = base[v] + (size_t)p * n, *c = base[v] + (size_t)q * n;
+    CK(cudaMemcpyAsync(tmp, a, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(a, c, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(c, tmp, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  return APHID_OK;
+}
+
+// AUTO, second phase: the escalated systems run the complex128 pass from
+// their current iterates, in as few chunks as device memory allows.  Each
+// chunk is moved to the front slots (the batched kernels address systems
+// 0..k-1), solved, and moved back.
+int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts *opts, const std::vector<int> &esc,
+                     std::vector<aphid_info> &out, long long &nlaunch) {
+  int rc = APHID_OK;
+  // the complex64 buffers are not needed again by this call: give their memory
+  // to the complex128 ones (the next mixed sweep re-allocates them)
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(ctx->sw_f32);
+  ctx->sw_f32 = nullptr;
+  ctx->sw_f32_ok = false;
+  double2 *tmp = nullptr;
+  if (cudaMalloc(&tmp, 2 * (size_t)ctx->n * sizeof(double2)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, APHID_ERR_NOMEM, "sweep: no memory to reorder escalated systems");
+  }
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const size_t per = 8 * 4 * (size_t)ctx->nl.N * sizeof(double2) + ((size_t)1 << 26);
+  const size_t have = fr + (ctx->sw_w64 ? (size_t)ctx->sw_nsys64 * 8 * 4 * ctx->nl.N * sizeof(double2) : 0);
+  const int cap = (int)std::max<size_t>(1, std::min<size_t>(esc.size(), (have - std::min(have, (size_t)1 << 30)) / per));
+  for (size_t c0 = 0; c0 < esc.size() && !rc; c0 += cap) {
+    const int k = (int)std::min<size_t>(cap, esc.size() - c0);
+    if ((rc = sweep_alloc64(ctx, k))) break;
+    // slot of each system, and the swaps that bring this chunk to the front
+    std::vector<int> slot_of(ctx->sw_nsys), sys_at(ctx->sw_nsys);
+    for (int q = 0; q < ctx->sw_nsys; q++) slot_of[q] = sys_at[q] = q;
+    std::vector<std::pair<int, int>> swaps;
+    for (int q = 0; q < k && !rc; q++) {
+      const int s = esc[c0 + q], p = slot_of[s];
+      if (p == q) continue;
+      rc = swap_systems(ctx, p, q, tmp);
+      swaps.push_back({p, q});
+      const int t = sys_at[q];
+      sys_at[q] = s;
+      sys_at[p] = t;
+      slot_of[s] = q;
+      slot_of[t] = p;
+    }
+    if (rc) break;
+    std::vector<SweepSys> h2(k);
+    for (int q = 0; q < k; q++) {
+      const int s = esc[c0 + q];
+      h2[q] = sweep_sys_init(omega[s], opts, true, false, std::max(1, opts->max_it - out[s].inner_iters));
+    }
+    SweepDev D2 = sweep_dev(ctx, k);
+    rc = run_batched(ctx, D2, true, h2, opts->max_it, nlaunch);
+    for (auto it = swaps.rbegin(); it != swaps.rend(); ++it) {
+      const int e = swap_systems(ctx, it->first, it->second, tmp);
+      if (!rc) rc = e;
+    }
+    if (rc) break;
+    for (int q = 0; q < k; q++) {
+      const int s = esc[c0 + q];
+      aphid_info I = sweep_info(h2[q], true);
+      I.iters += out[s].iters;
+      I.inner_iters += out[s].inner_iters;
+      I.outer_iters += out[s].outer_iters;
+      out[s] = I;
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(tmp);
+  // the complex128 buffers are sized for this phase only
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  return rc;
+}
+
+template <typename T>
+int sweep_apply_t(aphid_ctx *ctx, const aphid_z *x, aphid_z *y) {
+  int rc;
+  SweepDev D = sweep_dev(ctx, ctx->sw_last);
+  D.tmix = 0.f;
+  SweepSys S;
+  CK(cudaMemcpyAsync(&S, ctx->sw_sys, sizeof(SweepSys), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  S.vscale = 1.0;
+  S.beta = make_double2(0.0, 0.0);
+  S.k1 = make_double2(0.0, 0.0);
+  CK(cudaMemcpyAsync(ctx->sw_sys, &S, sizeof(SweepSys), cudaMemcpyHostToDevice, ctx->stream));
+  double2 *buf = nullptr;
+  CK(cudaMalloc(&buf, 2 * ctx->n * sizeof(double2)));
+  CK(cudaMemcpyAsync(buf, x, ctx->n * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  k_sw_apply_in<T><<<node_grid(ctx), 128, 0, ctx->stream>>>(D, buf);
+  if ((rc = pass_attrs(ctx))) {
+    cudaFree(buf);
+    return rc;
+  }
+  if (sizeof(T) == sizeof(double2))
+    launch_pass64(ctx, D, true);
+  else
+    launch_pass(ctx, D, true);
+  k_sw_apply_out<T><<<node_grid(ctx), 128, 0, ctx->stream>>>(D, buf + ctx->n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(y, buf + ctx->n, ctx->n * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(ctx, APHID_ERR_CUDA, cudaGetErrorString(e));
+  return APHID_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1102,14 +1383,18 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
   ctx->has_model = false;
   if (!ctx->d_sig) CK(cudaMalloc(&ctx->d_sig, ctx->n * sizeof(double)));
   if (!ctx->d_sig32) CK(cudaMalloc(&ctx->d_sig32, 4 * ctx->nl.N * sizeof(float)));
+  if (!ctx->d_sig64) CK(cudaMalloc(&ctx->d_sig64, 4 * ctx->nl.N * sizeof(double)));
   if (csig_flag != 'R') {
     if (!ctx->d_epsr) CK(cudaMalloc(&ctx->d_epsr, ctx->n * sizeof(double)));
     if (!ctx->d_epsr32) CK(cudaMalloc(&ctx->d_epsr32, 4 * ctx->nl.N * sizeof(float)));
+    if (!ctx->d_epsr64) CK(cudaMalloc(&ctx->d_epsr64, 4 * ctx->nl.N * sizeof(double)));
   } else {
     cudaFree(ctx->d_epsr);
     cudaFree(ctx->d_epsr32);
+    cudaFree(ctx->d_epsr64);
     ctx->d_epsr = nullptr;
     ctx->d_epsr32 = nullptr;
+    ctx->d_epsr64 = nullptr;
   }
   float *cells = nullptr;
   CK(cudaMalloc(&cells, ncell * sizeof(float)));
@@ -1124,10 +1409,14 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
     CK(cudaMemcpyAsync(cells, eps_rel, ncell * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
     k_sw_avg<<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_epsr);
     CK(cudaMemsetAsync(ctx->d_epsr32, 0, 4 * ctx->nl.N * sizeof(float), ctx->stream));
-    k_sw_to_node32<<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_epsr, ctx->d_epsr32);
+    k_sw_to_node<float><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_epsr, ctx->d_epsr32);
+    CK(cudaMemsetAsync(ctx->d_epsr64, 0, 4 * ctx->nl.N * sizeof(double), ctx->stream));
+    k_sw_to_node<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_epsr, ctx->d_epsr64);
   }
   CK(cudaMemsetAsync(ctx->d_sig32, 0, 4 * ctx->nl.N * sizeof(float), ctx->stream));
-  k_sw_to_node32<<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_sig, ctx->d_sig32);
+  k_sw_to_node<float><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_sig, ctx->d_sig32);
+  CK(cudaMemsetAsync(ctx->d_sig64, 0, 4 * ctx->nl.N * sizeof(double), ctx->stream));
+  k_sw_to_node<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_sig, ctx->d_sig64);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   cudaFree(cells);
@@ -1156,12 +1445,15 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
       return fail(ctx, APHID_ERR_BADARG, "source index out of range");
     if (!std::isfinite(omega[s])) return fail(ctx, APHID_ERR_BADARG, "non-finite omega");
   }
-  const bool mixed = opts->precision == APHID_PREC_MIXED;
-  if (!mixed && opts->precision != APHID_PREC_FP64) return fail(ctx, APHID_ERR_BADARG, "unknown precision");
+  const int prec = opts->precision;
+  const bool mixed = prec == APHID_PREC_MIXED || prec == APHID_PREC_AUTO;
+  const bool fused = prec == APHID_PREC_FUSED64;
+  if (!mixed && !fused && prec != APHID_PREC_FP64) return fail(ctx, APHID_ERR_BADARG, "unknown precision");
   if (!(opts->target >= 0.0) || opts->max_it < 0) return fail(ctx, APHID_ERR_BADARG, "bad target or max_it");
-  if (mixed && 4 * ctx->nl.N >= (1LL << 31))
-    return fail(ctx, APHID_ERR_BADARG, "mixed sweep: more than 2^31 node-layout values per system");
+  if ((mixed || fused) && 4 * ctx->nl.N >= (1LL << 31))
+    return fail(ctx, APHID_ERR_BADARG, "batched sweep: more than 2^31 node-layout values per system");
   if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
+  if (fused && (rc = sweep_alloc64(ctx, nsys))) return rc;
   if ((rc = ensure_work(ctx))) return rc;
   if (mixed) {
     if (ctx->plane_kz > 0) {
@@ -1202,58 +1494,20 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
     CK(cudaMemsetAsync(x64, 0, vec * sizeof(double2), ctx->stream));
 
   std::vector<SweepSys> hs(nsys);
-  for (int s = 0; s < nsys; s++) {
-    SweepSys &S = hs[s];
-    S = SweepSys{};
-    S.omega = omega[s];
-    S.ka = omega[s] * omega[s] * kMu0 * kEps0;
-    S.kb = omega[s] * kMu0;
-    S.target = opts->target;
-    S.max_it = opts->max_it;
-    S.inner_tol = opts->inner_tol > 0 ? opts->inner_tol : 1e-10;
-    S.max_outer = opts->max_outer > 0 ? opts->max_outer : 40;
-    S.phase = PH_OUTER;
-    S.status = -1;
-  }
-  CK(cudaMemcpyAsync(ctx->sw_sys, hs.data(), nsys * sizeof(SweepSys), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemsetAsync(ctx->sw_ndone, 0, sizeof(int), ctx->stream));
-  if (mixed) CK(cudaMemsetAsync(ctx->sw_err, 0, sizeof(int), ctx->stream));
+  for (int s = 0; s < nsys; s++) hs[s] = sweep_sys_init(omega[s], opts, fused, prec == APHID_PREC_AUTO, opts->max_it);
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   long long nlaunch = 0;
   std::vector<aphid_info> out(nsys);
 
-  if (mixed) {
-    k_sw_bnorm<<<(unsigned)(D.bps * nsys), kStreamThreads, 0, ctx->stream>>>(D);
-    CK(cudaGetLastError());
-    nlaunch += 1;
-    if ((rc = sweep_graph(ctx, D))) return rc;
-    const long long per_round = 3 + (long long)ctx->graph_iters;
-    const long long max_rounds = (long long)std::max(1, opts->max_it) / ctx->graph_iters + 2LL * (hs[0].max_outer + 2);
-    for (long long round = 0;; round++) {
-      CK(cudaMemcpyAsync(ctx->h_ndone, ctx->sw_ndone, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if (*ctx->h_ndone >= nsys) break;
-      if (round > max_rounds) return fail(ctx, APHID_ERR_STATE, "sweep did not terminate");
-      CK(cudaGraphLaunch(ctx->sw_gexec, ctx->stream));
-      nlaunch += per_round;
-    }
+  if (mixed || fused) {
+    if ((rc = run_batched(ctx, D, fused, hs, opts->max_it, nlaunch))) return rc;
+    for (int s = 0; s < nsys; s++) out[s] = sweep_info(hs[s], fused);
+    std::vector<int> esc;
+    for (int s = 0; s < nsys; s++)
+      if (hs[s].status == kStEscalated) esc.push_back(s);
+    if (!esc.empty() && (rc = finish_escalated(ctx, omega, opts, esc, out, nlaunch))) return rc;
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    CK(cudaMemcpyAsync(hs.data(), ctx->sw_sys, nsys * sizeof(SweepSys), cudaMemcpyDeviceToHost, ctx->stream));
-    int kerr = 0;
-    CK(cudaMemcpyAsync(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (kerr) return fail(ctx, APHID_ERR_CUDA, "sweep: a tensor-copy wait in the operator pass timed out");
-    for (int s = 0; s < nsys; s++) {
-      const SweepSys &S = hs[s];
-      aphid_info &I = out[s];
-      I.status = S.status;
-      I.iters = S.total_it;
-      I.inner_iters = S.total_it;
-      I.outer_iters = S.outer_it;
-      I.rhs_norm = S.bnorm;
-      I.recur_resid = S.tau;
-      I.true_rel_resid = S.bnorm > 0 ? S.rnorm / S.bnorm : S.rnorm;
-    }
   } else {
     // the reference's own algorithm, one system at a time, on resident data
     double2 *k2 = wv(ctx, W_K2), *dg = wv(ctx, W_INV);
@@ -1272,6 +1526,7 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
       CK(cudaMemcpyAsync(x64 + (size_t)s * ctx->n, wv(ctx, W_X), ctx->n * sizeof(double2),
                          cudaMemcpyDeviceToDevice, ctx->stream));
       nlaunch += 2 + I.kernel_launches;
+      I.inner64_iters = I.iters;
       out[s] = I;
     }
     ctx->loaded = false;
@@ -1288,6 +1543,7 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
     info[s] = out[s];
   }
   ctx->sw_last = nsys;
+  ctx->sw_last_fused = fused;
   if (x_out) {
     CK(cudaMemcpyAsync(x_out, x64, vec * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1298,12 +1554,18 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
 int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {
   int rc = check_ready(ctx);
   if (rc) return rc;
-  if (ctx->sw_last < 1 || !ctx->sw_f32_ok || reps < 1)
-    return fail(ctx, APHID_ERR_STATE, "no complex64 sweep state on the device");
+  const bool fused = ctx->sw_last_fused;
+  if (ctx->sw_last < 1 || reps < 1 || (fused ? (!ctx->sw_w64 || ctx->sw_nsys64 < ctx->sw_last) : !ctx->sw_f32_ok))
+    return fail(ctx, APHID_ERR_STATE, "no batched sweep state on the device");
   SweepDev D = sweep_dev(ctx, ctx->sw_last);
   D.tmix = 0.f;
   if ((rc = pass_attrs(ctx))) return rc;
-  for (int r = 0; r < reps; r++) launch_pass(ctx, D, true);
+  for (int r = 0; r < reps; r++) {
+    if (fused)
+      launch_pass64(ctx, D, true);
+    else
+      launch_pass(ctx, D, true);
+  }
   CK(cudaGetLastError());
   return APHID_OK;
 }
@@ -1311,6 +1573,20 @@ int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {
 int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx) {
   if (!ctx) return APHID_ERR_BADARG;
   return ctx->sw_work ? ctx->ptiles.kz : 0;
+}
+
+int aphid_gpu_sweep_apply(aphid_ctx *ctx, const aphid_z *x, aphid_z *y) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!x || !y) return fail(ctx, APHID_ERR_BADARG, "null vector");
+  if (ctx->sw_last < 1) return fail(ctx, APHID_ERR_STATE, "no batched sweep state on the device");
+  if (ctx->sw_last_fused) {
+    if (!ctx->sw_w64 || ctx->sw_nsys64 < ctx->sw_last)
+      return fail(ctx, APHID_ERR_STATE, "no complex128 sweep state on the device");
+    return sweep_apply_t<double2>(ctx, x, y);
+  }
+  if (!ctx->sw_f32_ok) return fail(ctx, APHID_ERR_STATE, "no complex64 sweep state on the device");
+  return sweep_apply_t<float2>(ctx, x, y);
 }
 
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x) {

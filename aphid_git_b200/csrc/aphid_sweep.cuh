@@ -64,6 +64,11 @@ constexpr int kParts = 12;  // partial sums per slot and system
 // recurrence has reached its floor and only a restart from the FP64 residual
 // makes progress.
 constexpr double kStagnation = 16.0;
+// The monitor runs only once the quasi-residual predicts a true residual
+// (rnorm at the cycle start times tau / tau0) below this fraction of ||b||,
+// or below 30 x the target: above both, neither convergence nor the
+// complex64 floor (about 1e-6 ||b||) can have been reached.
+constexpr double kMonitorLevel = 1e-4;
 // rho_{n+1}^2 from the expansion ||q||^2 - 2 Re(conj(beta) v^H q) + |beta|^2
 // ||v||^2 is trusted down to this fraction of ||q||^2; below it the new
 // Lanczos vector is treated as zero (the iterate is final for this cycle).
@@ -71,6 +76,23 @@ constexpr double kCancel = 1e-10;
 // the cycle also restarts when the stored v~_n has drifted from ||v~_n|| = 1
 // or from v~_n^T v~_n = delta_n by more than this (relative to ||v~_n||^2)
 constexpr double kDrift = 1e-3;
+// A cycle whose quasi-residual has not halved over this many iterations (the
+// default of SweepSys::stall_window) has stalled: the complex64 Lanczos
+// process can stagnate outright (seen on seafloor models at 0.27-1.35 Hz,
+// where complex128 converges in about 500 iterations).  The cycle ends and
+// the next one restarts from the FP64 residual.
+constexpr int kStallWindow = 400;
+// Complex-symmetric Lanczos normalises v~ in the Hermitian norm but divides by
+// the bilinear form delta = v~^T v~.  On strongly conducting layers under air
+// |delta| / ||v~||^2 falls to 1e-7 and below within a few dozen iterations
+// (seafloor models, 0.27-1.35 Hz), where complex64 storage noise (about 6e-8
+// of ||v~||^2) is a sizeable part of delta: the complex64 process loses
+// biorthogonality and stalls, while complex128 converges.  With escalation on,
+// a system whose |delta_{n+1}| falls below this fraction of ||v~_n||^2 ends
+// with kStEscalated and is finished by the complex128 pass (k_sw_pass64).
+// Heterogeneous land models stay above 1e-5.
+constexpr double kDeltaFloor = 1e-6;
+constexpr int kStEscalated = 4;
 
 struct SweepSys {
   double omega, ka, kb;  // k^2 = (-ka * eps-bar, kb * sigma-bar)
@@ -84,7 +106,12 @@ struct SweepSys {
   int phase, has_inner, inner_it, total_it, outer_it, max_it, max_outer, status;
   int checks, pending;
   int cur;                   // buffer set holding q^, v^, p^ of the last pass
-  int restarts;              // inner cycles ended by kCancel / kDrift
+  int restarts;              // inner cycles ended by kCancel / kDrift / a stall
+  double tau_win;            // tau at the start of the current stall window
+  int win_it;                // inner iteration at which that window started
+  int stall_window;          // window length (INT_MAX: no stall test)
+  int escalate;              // 1: end with kStEscalated when the bilinear form collapses
+  int escalated;             // set by the pass; the outer step then ends the system
 };
 
 // plane tile of the complex64 pass: 16 x 16 nodes marching along k; staged
@@ -122,10 +149,21 @@ struct SweepDev {
   float tmix;                    // 1; 0 in timing launches (d^, x^ rewritten unchanged)
   int *work;                     // [2]: next work item, blocks finished (complex64 pass)
   const int *order;              // plane tiles in the order the pass takes them
+  // complex128 inner storage (k_sw_pass64): same layouts, double2
+  double2 *W64, *dd64, *xx64;
+  const double *sig64, *epsr64;  // sigma-bar / eps-bar, FP64, node layout [4][N]
+  const double4 *ax64;           // the axis tables of ax32 in FP64
 };
 
 __device__ __forceinline__ float2 *wvec(const SweepDev &D, int set, int sys, int vec) {
   return D.W + ((long long)(set * D.nsys + sys) * 3 + vec) * 4 * D.L.N;
+}
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+  const double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ double2 *wvec64(const SweepDev &D, int set, int sys, int vec) {
+  return D.W64 + ((long long)(set * D.nsys + sys) * 3 + vec) * 4 * D.L.N;
 }
 __device__ __forceinline__ long long nd_of(const SweepDev &D, int i, int j, int k) {
   return i + (long long)D.L.nxp * (j + (long long)D.g.ny * k);
@@ -195,6 +233,53 @@ __device__ __forceinline__ void jacobi_weights(float2 z, float2 &inv, float &abs
     inv = make_float2(__fmul_rn(za, t), -__fmul_rn(zb, t));
     absd = __fmul_rn(__fmul_rn(mz, n2), rn);
     rabsd = __fmul_rn(sc, rn);
+  }
+}
+
+// The same two functions in FP64 for the complex128 pass (k_sw_pass64) and
+// the kernels that share its state: the diagonal of K from the FP64 axis
+// tables and sigma-bar, and D^-1, |D|, 1/|D| -- all with non-contracting
+// intrinsics so that every kernel forms bit-identical values.
+__device__ __forceinline__ void jacobi64(double4 XA, double4 XB, double4 YA, double4 YB, double4 ZA, double4 ZB,
+                                         double sx, double sy, double sz, double sp0, double sxm, double sym,
+                                         double s2m, double ex, double ey, double ez, double ep0, double exm,
+                                         double eym, double e2m, bool hx, bool hy, bool hz, bool pin, double ka,
+                                         double kb, double2 dg[4]) {
+  auto M = [](double a, double b) { return __dmul_rn(a, b); };
+  auto A = [](double a, double b) { return __dadd_rn(a, b); };
+  auto edge = [&](double vol, double sum, double s_, double e_) {
+    return make_double2(M(vol, __dsub_rn(-M(ka, e_), sum)), M(vol, M(kb, s_)));
+  };
+  const double xn4 = XA.x, xn5 = XA.y, dxc = XA.z, yn4 = YA.x, yn5 = YA.y, dyc = YA.z, zn4 = ZA.x, zn5 = ZA.y,
+               dzc = ZA.z;
+  dg[0] = hx ? edge(M(M(XB.z, dyc), dzc), A(A(A(A(A(XB.x, XB.y), yn4), yn5), zn4), zn5), sx, ex)
+             : make_double2(0.0, 0.0);
+  dg[1] = hy ? edge(M(M(dxc, YB.z), dzc), A(A(A(A(A(YB.x, YB.y), xn4), xn5), zn4), zn5), sy, ey)
+             : make_double2(0.0, 0.0);
+  dg[2] = hz ? edge(M(M(dxc, dyc), ZB.z), A(A(A(A(A(ZB.x, ZB.y), xn4), xn5), yn4), yn5), sz, ez)
+             : make_double2(0.0, 0.0);
+  if (pin) {
+    const double vol = M(M(dxc, dyc), dzc);
+    const double s1r = -M(ka, ep0), s1i = M(kb, sp0);
+    const double nr = A(A(A(A(A(M(xn4, ex), M(xn5, exm)), M(yn4, ey)), M(yn5, eym)), M(zn4, ez)), M(zn5, e2m));
+    const double ni = A(A(A(A(A(M(xn4, sx), M(xn5, sxm)), M(yn4, sy)), M(yn5, sym)), M(zn4, sz)), M(zn5, s2m));
+    const double pr = __dsub_rn(M(s1r, s1r), M(s1i, s1i)), pi = M(2.0, M(s1r, s1i));
+    dg[3] = make_double2(M(vol, A(pr, M(ka, nr))), M(vol, __dsub_rn(pi, M(kb, ni))));
+  } else {
+    dg[3] = make_double2(1.0, 0.0);
+  }
+}
+__device__ __forceinline__ void jacobi_weights(double2 z, double2 &inv, double &absd, double &rabsd) {
+  const double mz = fmax(fabs(z.x), fabs(z.y));
+  inv = make_double2(0.0, 0.0);
+  absd = rabsd = 0.0;
+  if (mz > 0.0) {
+    const double sc = __ddiv_rn(1.0, mz), za = __dmul_rn(z.x, sc), zb = __dmul_rn(z.y, sc);
+    const double n2 = __dadd_rn(__dmul_rn(za, za), __dmul_rn(zb, zb)), rn = __ddiv_rn(1.0, __dsqrt_rn(n2));
+    const double t = __dmul_rn(sc, __dmul_rn(rn, rn));
+    inv = make_double2(__dmul_rn(za, t), -__dmul_rn(zb, t));
+    absd = __dmul_rn(__dmul_rn(mz, n2), rn);
+    rabsd = __dmul_rn(sc, rn);
   }
 }
 
@@ -298,10 +383,11 @@ struct K2Ref64 {  // k^2 from the FP64 averages (reference layout)
     return make_double2(-ka * e, kb * __ldg(sig + t));
   }
 };
-struct XRef64 {  // x (reference layout), optionally + x^ (node layout)
+template <typename T>
+struct XRefT {  // x (reference layout), optionally + x^ (node layout, complex64 or complex128)
   GridDev g;
   const double2 *__restrict__ x64;
-  const float2 *__restrict__ xt;  // null: x only
+  const T *__restrict__ xt;  // null: x only
   int nxp;
   long long N;
   __device__ __forceinline__ double2 operator()(int c, int i, int j, int k) const {
@@ -310,6 +396,7 @@ struct XRef64 {  // x (reference layout), optionally + x^ (node layout)
     return r;
   }
 };
+using XRef64 = XRefT<float2>;
 
 __device__ __forceinline__ void sweep_tile(const SweepDev &D, long long tile, int &i, int &j, int &k0,
                                            int &k1) {
@@ -421,14 +508,14 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_bnorm(SweepDev D) 
 
 // reference-layout FP64 per-unknown array -> node-layout FP32 [4][N]
 // (zero where a component does not exist; pads are left as initialised)
-static __global__ void k_sw_to_node32(GridDev g, NodeLayout L, const double *__restrict__ ref,
-                                      float *__restrict__ node) {
+template <typename F>
+static __global__ void k_sw_to_node(GridDev g, NodeLayout L, const double *__restrict__ ref, F *__restrict__ node) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
   const long long nd = i + (long long)L.nxp * (j + (long long)g.ny * k);
 #pragma unroll
   for (int c = 0; c < 4; c++)
-    node[c * L.N + nd] = exists(g, c, i, j, k) ? (float)ref[ref_of(g, c, i, j, k)] : 0.f;
+    node[c * L.N + nd] = exists(g, c, i, j, k) ? (F)ref[ref_of(g, c, i, j, k)] : (F)0;
 }
 
 
@@ -446,6 +533,116 @@ static __global__ void k_sw_axis32(GridDev g, float4 *out) {
   out[base + n + m] = make_float4(e ? (float)A.e2[m] : 0.f, e ? (float)A.e3[m] : 0.f, e ? (float)A.d[m + 1] : 1.f,
                                   e ? (float)(1.0 / A.d[m + 1]) : 1.f);
 }
+// the same tables in FP64 (complex128 pass)
+static __global__ void k_sw_axis64(GridDev g, double4 *out) {
+  const int a = blockIdx.y;
+  const Axis A = a == 0 ? g.ax[0] : (a == 1 ? g.ax[1] : g.ax[2]);
+  const int n = A.n, m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const int base = a == 0 ? 0 : (a == 1 ? 2 * g.ax[0].n : 2 * (g.ax[0].n + g.ax[1].n));
+  out[base + m] = make_double4(A.n4[m], A.n5[m], A.dc[m], 1.0 / A.dc[m]);
+  const bool e = m < n - 1;
+  out[base + n + m] = make_double4(e ? A.e2[m] : 0.0, e ? A.e3[m] : 0.0, e ? A.d[m + 1] : 1.0, e ? 1.0 / A.d[m + 1] : 1.0);
+}
+
+
+// O2: r = b - K x in complex128 (true residual).  The next inner cycle starts
+// from r~_0 = D^-1/2 r (D from jacobi32, as in the pass), stored as
+// q^ = D^-1 r with v^ = p^ = d^ = x^ = 0 and
+// beta_0 = 0, so that the first pass forms v~_1 = r~_0 / ||r~_0||; scalars of
+// src/aphid_qmr.f90:268-285, 299-313 with M = I.
+// The Jacobi diagonal of node (i, j, k) exactly as the complex64 pass forms
+// it (the same function on the same FP32 values)
+__device__ __forceinline__ void node_diag32(const SweepDev &D, const SweepSys *S, int i, int j, int k, float2 dg[4]) {
+  const int nx = D.g.nx, ny = D.g.ny, nz = D.g.nz;
+  const long long N = D.L.N, plane = (long long)D.L.nxp * ny, nd = nd_of(D, i, j, k);
+  const float4 *AX = D.ax32, *AY = D.ax32 + 2 * nx, *AZ = D.ax32 + 2 * (nx + ny);
+  auto sg = [&](int c, long long q) { return __ldg(D.sig32 + c * N + q); };
+  auto ep = [&](int c, long long q) { return D.epsr32 ? __ldg(D.epsr32 + c * N + q) : 1.f; };
+  const bool pin = i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1;
+  jacobi32(__ldg(AX + i), __ldg(AX + nx + i), __ldg(AY + j), __ldg(AY + ny + j), __ldg(AZ + k), __ldg(AZ + nz + k),
+           sg(0, nd), sg(1, nd), sg(2, nd), sg(3, nd), pin ? sg(0, nd - 1) : 0.f, pin ? sg(1, nd - D.L.nxp) : 0.f,
+           pin ? sg(2, nd - plane) : 0.f, ep(0, nd), ep(1, nd), ep(2, nd), ep(3, nd), pin ? ep(0, nd - 1) : 1.f,
+           pin ? ep(1, nd - D.L.nxp) : 1.f, pin ? ep(2, nd - plane) : 1.f, i < nx - 1, j < ny - 1, k < nz - 1, pin,
+           (float)S->ka, (float)S->kb, dg);
+}
+// ... and the complex128 pass's diagonal from the FP64 tables
+__device__ __forceinline__ void node_diag64(const SweepDev &D, const SweepSys *S, int i, int j, int k,
+                                            double2 dg[4]) {
+  const int nx = D.g.nx, ny = D.g.ny, nz = D.g.nz;
+  const long long N = D.L.N, plane = (long long)D.L.nxp * ny, nd = nd_of(D, i, j, k);
+  const double4 *AX = D.ax64, *AY = D.ax64 + 2 * nx, *AZ = D.ax64 + 2 * (nx + ny);
+  auto sg = [&](int c, long long q) { return __ldg(D.sig64 + c * N + q); };
+  auto ep = [&](int c, long long q) { return D.epsr64 ? __ldg(D.epsr64 + c * N + q) : 1.0; };
+  const bool pin = i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1;
+  jacobi64(ldg4(AX + i), ldg4(AX + nx + i), ldg4(AY + j), ldg4(AY + ny + j), ldg4(AZ + k), ldg4(AZ + nz + k),
+           sg(0, nd), sg(1, nd), sg(2, nd), sg(3, nd), pin ? sg(0, nd - 1) : 0.0, pin ? sg(1, nd - D.L.nxp) : 0.0,
+           pin ? sg(2, nd - plane) : 0.0, ep(0, nd), ep(1, nd), ep(2, nd), ep(3, nd), pin ? ep(0, nd - 1) : 1.0,
+           pin ? ep(1, nd - D.L.nxp) : 1.0, pin ? ep(2, nd - plane) : 1.0, i < nx - 1, j < ny - 1, k < nz - 1, pin,
+           S->ka, S->kb, dg);
+}
+
+// Inner storage of a sweep: complex64 (k_sw_pass) or complex128 (k_sw_pass64)
+template <typename T> struct Inner;
+template <> struct Inner<float2> {
+  using R = float;
+  static __device__ __forceinline__ float2 *vec(const SweepDev &D, int set, int sys, int v) {
+    return wvec(D, set, sys, v);
+  }
+  static __device__ __forceinline__ float2 *dd(const SweepDev &D) { return D.dd; }
+  static __device__ __forceinline__ float2 *xx(const SweepDev &D) { return D.xx; }
+  static __device__ __forceinline__ void diag(const SweepDev &D, const SweepSys *S, int i, int j, int k,
+                                              float2 dg[4]) {
+    node_diag32(D, S, i, j, k, dg);
+  }
+  static __device__ __forceinline__ float2 from_d(double2 a) { return to_f(a); }
+};
+template <> struct Inner<double2> {
+  using R = double;
+  static __device__ __forceinline__ double2 *vec(const SweepDev &D, int set, int sys, int v) {
+    return wvec64(D, set, sys, v);
+  }
+  static __device__ __forceinline__ double2 *dd(const SweepDev &D) { return D.dd64; }
+  static __device__ __forceinline__ double2 *xx(const SweepDev &D) { return D.xx64; }
+  static __device__ __forceinline__ void diag(const SweepDev &D, const SweepSys *S, int i, int j, int k,
+                                              double2 dg[4]) {
+    node_diag64(D, S, i, j, k, dg);
+  }
+  static __device__ __forceinline__ double2 from_d(double2 a) { return a; }
+};
+
+// Test hook (aphid_gpu_sweep_apply32): x (reference layout, complex128) as
+// the q^ of system 0's read set, with v^ = p^ = 0, so that a timing pass with
+// vscale 1, beta 0, k1 0 forms u = x and q^ = D^-1 K u
+template <typename T>
+static __global__ void k_sw_apply_in(SweepDev D, const double2 *__restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= D.g.nx) return;
+  const int cur = D.sys->cur;
+  T *Q = Inner<T>::vec(D, cur, 0, 0), *V = Inner<T>::vec(D, cur, 0, 1), *P = Inner<T>::vec(D, cur, 0, 2);
+  const long long nd = nd_of(D, i, j, k);
+  const T zero = Inner<T>::from_d(make_double2(0.0, 0.0));
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const long long t = c * D.L.N + nd;
+    Q[t] = exists(D.g, c, i, j, k) ? Inner<T>::from_d(x[ref_of(D.g, c, i, j, k)]) : zero;
+    V[t] = zero;
+    P[t] = zero;
+  }
+}
+// ... and y = D q^ of the set that pass wrote (reference layout, complex128)
+template <typename T>
+static __global__ void k_sw_apply_out(SweepDev D, double2 *__restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= D.g.nx) return;
+  const T *Q = Inner<T>::vec(D, D.sys->cur, 0, 0);
+  T dg[4];
+  Inner<T>::diag(D, D.sys, i, j, k, dg);
+  const long long nd = nd_of(D, i, j, k);
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+    if (exists(D.g, c, i, j, k)) y[ref_of(D.g, c, i, j, k)] = cmul(to_d(dg[c]), to_d(Q[c * D.L.N + nd]));
+}
 
 // ------------------------------------------------------------ outer step
 // O1: x += x^ (+ the pending lagged update), FP64 accumulation of the inner
@@ -454,6 +651,7 @@ static __global__ void k_sw_axis32(GridDev g, float4 *out) {
 // x and zeroes it, leaving the pending update pending: x^ then only ever
 // holds the last round's increments, so its complex64 rounding no longer
 // sets the floor of the cycle (about 8x lower on the test meshes).
+template <typename T>
 static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
   const int sys = blockIdx.x % D.nsys, chunk = blockIdx.x / D.nsys;
   const SweepSys *S = D.sys + sys;
@@ -463,8 +661,8 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
   const bool pend = !flush && S->pending != 0;
   const double2 eta = S->eta_pend;
   const double kap = S->kap_pend;
-  const float2 *P = wvec(D, S->cur, sys, 2), *dd = D.dd + vb;
-  float2 *xx = D.xx + vb;
+  const T *P = Inner<T>::vec(D, S->cur, sys, 2), *dd = Inner<T>::dd(D) + vb;
+  T *xx = Inner<T>::xx(D) + vb;
   const GridDev &g = D.g;
   const long long plane = (long long)D.L.nxp * g.ny;
   double2 *x64 = D.x64 + (long long)sys * D.n;
@@ -482,16 +680,12 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
       if (pend) xt = cadd(xt, cadd(cmul(eta, to_d(P[t])), rmul(kap, to_d(dd[t]))));
       const long long rt = ref_of(g, c, i, j, k);
       x64[rt] = cadd(x64[rt], xt);
-      if (flush) xx[t] = make_float2(0.f, 0.f);
+      if (flush) xx[t] = Inner<T>::from_d(make_double2(0.0, 0.0));
     }
   }
 }
 
-// O2: r = b - K x in complex128 (true residual).  The next inner cycle starts
-// from r~_0 = D^-1/2 r (D from jacobi32, as in the pass), stored as
-// q^ = D^-1 r with v^ = p^ = d^ = x^ = 0 and
-// beta_0 = 0, so that the first pass forms v~_1 = r~_0 / ||r~_0||; scalars of
-// src/aphid_qmr.f90:268-285, 299-313 with M = I.
+template <typename T>
 static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
   const int sys = blockIdx.x % D.nsys;
   const long long tile = blockIdx.x / D.nsys;
@@ -505,37 +699,26 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
     const K2Ref64 K{D.g, D.sig, D.epsr, S->ka, S->kb};
     const double2 *b = D.b + (long long)sys * D.n;
     const long long vb = (long long)sys * 4 * D.L.N;
-    float2 *Q = wvec(D, S->cur, sys, 0), *V = wvec(D, S->cur, sys, 1), *P = wvec(D, S->cur, sys, 2);
-    const float2 zero = make_float2(0.f, 0.f);
-    const int nx = D.g.nx, ny = D.g.ny, nz = D.g.nz;
-    const long long N = D.L.N, plane = (long long)D.L.nxp * ny;
-    const float4 *AX = D.ax32, *AY = D.ax32 + 2 * nx, *AZ = D.ax32 + 2 * (nx + ny);
-    const float4 XA = __ldg(AX + i), XB = __ldg(AX + nx + i), YA = __ldg(AY + j), YB = __ldg(AY + ny + j);
-    const float ka = (float)S->ka, kb = (float)S->kb;
-    auto sg = [&](int c, long long nd) { return __ldg(D.sig32 + c * N + nd); };
-    auto ep = [&](int c, long long nd) { return D.epsr32 ? __ldg(D.epsr32 + c * N + nd) : 1.f; };
+    T *Q = Inner<T>::vec(D, S->cur, sys, 0), *V = Inner<T>::vec(D, S->cur, sys, 1),
+      *P = Inner<T>::vec(D, S->cur, sys, 2), *dd = Inner<T>::dd(D), *xx = Inner<T>::xx(D);
+    using R = typename Inner<T>::R;
+    const T zero = Inner<T>::from_d(make_double2(0.0, 0.0));
     for (int k = k0; k < k1; k++) {
       double2 o[4];
       rowsN<double>(D.g, i, j, k, L, K, o);
       const long long nd = nd_of(D, i, j, k);
-      // the Jacobi diagonal exactly as the complex64 pass forms it
-      const bool pin = i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1;
-      float2 dg[4];
-      jacobi32(XA, XB, YA, YB, __ldg(AZ + k), __ldg(AZ + nz + k), sg(0, nd), sg(1, nd), sg(2, nd), sg(3, nd),
-               pin ? sg(0, nd - 1) : 0.f, pin ? sg(1, nd - D.L.nxp) : 0.f, pin ? sg(2, nd - plane) : 0.f,
-               ep(0, nd), ep(1, nd), ep(2, nd), ep(3, nd), pin ? ep(0, nd - 1) : 1.f,
-               pin ? ep(1, nd - D.L.nxp) : 1.f, pin ? ep(2, nd - plane) : 1.f, i < nx - 1, j < ny - 1, k < nz - 1,
-               pin, ka, kb, dg);
+      T dg[4];
+      Inner<T>::diag(D, S, i, j, k, dg);
 #pragma unroll
       for (int c = 0; c < 4; c++) {
         const long long t = c * D.L.N + nd;
-        float2 rq = zero;
+        T rq = zero;
         if (exists(D.g, c, i, j, k)) {
           const double2 r = csub(b[ref_of(D.g, c, i, j, k)], o[c]);
-          float2 inv;
-          float absd, rabsd;
+          T inv;
+          R absd, rabsd;
           jacobi_weights(dg[c], inv, absd, rabsd);
-          rq = to_f(cmul(to_d(inv), r));
+          rq = Inner<T>::from_d(cmul(to_d(inv), r));
           a.v[0] += cabs2(r);
           const double2 q = to_d(rq);
           a.v[1] += (double)absd * cabs2(q);         // ||r~||^2 = sum |D| |q^|^2
@@ -546,8 +729,8 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
         Q[t] = rq;
         V[t] = zero;
         P[t] = zero;
-        D.dd[vb + t] = zero;
-        D.xx[vb + t] = zero;
+        dd[vb + t] = zero;
+        xx[vb + t] = zero;
       }
     }
   }
@@ -565,6 +748,8 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
         mark_done(D, S, 3);
       } else if (S->rnorm < S->target * S->bnorm) {
         mark_done(D, S, 0);
+      } else if (S->escalated) {
+        mark_done(D, S, kStEscalated);
       } else if (S->outer_it >= S->max_outer || S->total_it >= S->max_it) {
         mark_done(D, S, 1);
       } else {
@@ -584,6 +769,8 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
         S->del = rmul(S->vscale * S->vscale, make_double2(tot.v[2], tot.v[3]));
         S->k1 = cdiv(rmul(S->rho_n, S->del), S->eps);
         S->tau = S->tau0 = rt0;
+        S->tau_win = rt0;
+        S->win_it = 0;
         S->ratio_min = 1e300;
         S->inner_it = 0;
         S->has_inner = 1;
@@ -597,21 +784,24 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
 }
 
 // Monitor: the true residual of the running iterate, ||b - K (x + x^)|| in
-// complex128 (x^ lags one update), once per graph round.  Ends the inner
+// complex128 (x^ lags one update), once per graph round once the cycle is
+// near its end (see kMonitorLevel).  Ends the inner
 // cycle on convergence or on stagnation of the complex64 recurrence (see
 // kStagnation); the next round's outer step folds x^ into x and restarts
 // from the FP64 residual.
+template <typename T>
 static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
   const int sys = blockIdx.x % D.nsys;
   const long long tile = blockIdx.x / D.nsys;
   SweepSys *S = D.sys + sys;
   if (S->phase != PH_INNER || S->inner_it < 2) return;
+  if (S->rnorm * (S->tau / S->tau0) > fmax(kMonitorLevel, 30.0 * S->target) * S->bnorm) return;
   int i, j, k0, k1;
   sweep_tile(D, tile, i, j, k0, k1);
   Vals<1> a{{0.0}};
   if (i < D.g.nx && j < D.g.ny) {
     const long long vb = (long long)sys * 4 * D.L.N;
-    const XRef64 L{D.g, D.x64 + (long long)sys * D.n, D.xx + vb, D.L.nxp, D.L.N};
+    const XRefT<T> L{D.g, D.x64 + (long long)sys * D.n, Inner<T>::xx(D) + vb, D.L.nxp, D.L.N};
     const K2Ref64 K{D.g, D.sig, D.epsr, S->ka, S->kb};
     const double2 *b = D.b + (long long)sys * D.n;
     for (int k = k0; k < k1; k++) {
@@ -686,6 +876,7 @@ struct PassMaps {
   CUtensorMap w;         // 5-D: (nxp, ny, nz, vector x component = 12, set x system), 8-byte elements
   CUtensorMap sig, eps;  // 4-D: (nxp, ny, nz, component), FP32
   CUtensorMap dd, xx;    // 5-D: (nxp, ny, nz, component, system), 8-byte elements
+  CUtensorMap w64;       // complex128 q^ v^ p^: 5-D (2 nxp, ny, nz, 12, set x system), 8-byte elements
 };
 
 constexpr int kStages = 3;                       // load ring depth of the pass
@@ -832,7 +1023,15 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T) {
   // delta, which may be small in complex-symmetric Lanczos without any loss
   const bool drift = fabs(A3 - 1.0) > kDrift || sqrt(cabs2(csub(B3, S->del))) > kDrift * A3;
   if (drift) S->restarts++;
-  if (!S->pending || !isfinite(S->tau) || !finite2(del) || zero2(del) || drift ||
+  bool stall = false;
+  if (S->inner_it - S->win_it >= S->stall_window) {
+    stall = S->tau > 0.5 * S->tau_win;
+    S->tau_win = S->tau;
+    S->win_it = S->inner_it;
+  }
+  if (stall) S->restarts++;
+  if (S->escalate && sqrt(cabs2(del)) < kDeltaFloor * A3) S->escalated = 1;
+  if (S->escalated || !S->pending || !isfinite(S->tau) || !finite2(del) || zero2(del) || drift || stall ||
       S->tau < S->inner_tol * S->tau0 || S->total_it >= S->max_it) {
     S->phase = PH_OUTER;
     return;
@@ -1182,6 +1381,381 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
   }
   }  // work items
   // the last block out re-arms the work counter for the next launch
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(D.work + 1, 1) == gridDim.x - 1) {
+      D.work[0] = 0;
+      D.work[1] = 0;
+      __threadfence();
+    }
+  }
+}
+
+
+// ------------------------------------------------------------ complex128 pass
+// k_sw_pass64: the fused QMR iteration of k_sw_pass with complex128 vectors,
+// FP64 coefficients (sigma-bar, eps-bar, axis tables) and FP64 arithmetic, for
+// systems on which complex64 storage cannot carry the Lanczos process (see
+// kDeltaFloor).  Same tiles, same work order, same inner products and scalar
+// step (pass_scalars); 2 TMA stages of q^ v^ p^ planes (69 KB each); sigma-bar
+// and d^, x^ are read with plain loads.
+constexpr int kStages64 = 2;
+constexpr unsigned kRawBytes64 = 12u * kPN * 16u;  // q^, v^, p^ with halo, four components, complex128
+constexpr unsigned kUBytes64 = 4u * kPN * 16u;
+constexpr size_t kPass64Shm = kStages64 * (size_t)kRawBytes64 + 2 * (size_t)kUBytes64 + 128;
+
+__device__ __forceinline__ double2 daxpy(double a, double2 x, double2 y) {
+  return make_double2(fma(a, x.x, y.x), fma(a, x.y, y.y));
+}
+__device__ __forceinline__ double2 dcfma(double2 a, double2 x, double2 y) {  // y + a x
+  return make_double2(fma(a.x, x.x, fma(-a.y, x.y, y.x)), fma(a.x, x.y, fma(a.y, x.x, y.y)));
+}
+// the rows of edge_row / edge_row_c / node_row / node_row_c in FP64
+__device__ __forceinline__ double2 edge_row64(double2 u0, double2 n1, double c1, double2 n2, double c2, double2 n3,
+                                              double c3, double2 n4, double c4, double2 n5, double c5, double2 n6,
+                                              double c6, double s0, double spn, double sp0, double2 f1, double2 f0,
+                                              double rd, double vol, double ka, double kb) {
+  const double2 t1 = daxpy(c2, csub(n2, u0), rmul(c1, csub(n1, u0)));
+  const double2 t2 = daxpy(c4, csub(n4, u0), rmul(c3, csub(n3, u0)));
+  const double2 t3 = daxpy(c6, csub(n6, u0), rmul(c5, csub(n5, u0)));
+  const double2 L = cadd(cadd(t1, t2), daxpy(-ka, u0, t3));
+  const double2 M = daxpy(rd * (spn - sp0), f0, daxpy(rd * (spn - s0), csub(f1, f0), rmul(s0, u0)));
+  return make_double2(vol * (L.x - kb * M.y), vol * (L.y + kb * M.x));
+}
+__device__ __forceinline__ double2 edge_row64_c(double2 u0, double2 n1, double c1, double2 n2, double c2,
+                                                double2 n3, double c3, double2 n4, double c4, double2 n5, double c5,
+                                                double2 n6, double c6, double2 k2, double2 kpn, double2 kp0,
+                                                double2 f1, double2 f0, double rd, double vol) {
+  const double2 t1 = daxpy(c2, csub(n2, u0), rmul(c1, csub(n1, u0)));
+  const double2 t2 = daxpy(c4, csub(n4, u0), rmul(c3, csub(n3, u0)));
+  const double2 t3 = daxpy(c6, csub(n6, u0), rmul(c5, csub(n5, u0)));
+  const double2 g = dcfma(rmul(rd, csub(kpn, kp0)), f0, dcfma(rmul(rd, csub(kpn, k2)), csub(f1, f0), cmul(k2, u0)));
+  const double2 L = cadd(cadd(t1, t2), cadd(t3, g));
+  return rmul(vol, L);
+}
+__device__ __forceinline__ double2 node_row64(double2 f, double2 fxp, double2 fxm, double2 fyp, double2 fym,
+                                              double2 fzp, double2 fzm, double xn4, double xn5, double yn4,
+                                              double yn5, double zn4, double zn5, double2 a0, double2 a0m,
+                                              double2 a1, double2 a1m, double2 a2, double2 a2m, double rdxc,
+                                              double rdyc, double rdzc, double sx, double sxm, double sy, double sym,
+                                              double sz, double szm, double sp0, double vol, double ka, double kb) {
+  const double2 g1 = csub(fxp, f), g2 = csub(fxm, f), g3 = csub(fyp, f), g4 = csub(fym, f), g5 = csub(fzp, f),
+                g6 = csub(fzm, f);
+  const double2 T1 = cadd(cadd(daxpy(xn5, g2, rmul(xn4, g1)), daxpy(yn5, g4, rmul(yn4, g3))),
+                          daxpy(zn5, g6, rmul(zn4, g5)));
+  const double2 T2a = cadd(daxpy(xn5 * sxm, g2, rmul(xn4 * sx, g1)), daxpy(yn5 * sym, g4, rmul(yn4 * sy, g3)));
+  const double2 T2b = daxpy(zn5 * szm, g6, rmul(zn4 * sz, g5));
+  const double2 Ea = daxpy(rdxc * (sx - sxm), a0m, rmul(rdxc * (sx - sp0), csub(a0, a0m)));
+  const double2 Eb = daxpy(rdyc * (sy - sym), a1m, rmul(rdyc * (sy - sp0), csub(a1, a1m)));
+  const double2 Ec = daxpy(rdzc * (sz - szm), a2m, rmul(rdzc * (sz - sp0), csub(a2, a2m)));
+  const double2 T2 = cadd(cadd(T2a, T2b), cadd(cadd(Ea, Eb), Ec));
+  const double2 t = dcfma(make_double2(ka * ka - kb * kb * sp0 * sp0, -2.0 * ka * kb * sp0), f,
+                          make_double2(-ka * T1.x, -ka * T1.y));
+  return make_double2(vol * (t.x - kb * T2.y), vol * (t.y + kb * T2.x));
+}
+__device__ __forceinline__ double2 node_row64_c(double2 f, double2 fxp, double2 fxm, double2 fyp, double2 fym,
+                                                double2 fzp, double2 fzm, double xn4, double xn5, double yn4,
+                                                double yn5, double zn4, double zn5, double2 a0, double2 a0m,
+                                                double2 a1, double2 a1m, double2 a2, double2 a2m, double rdxc,
+                                                double rdyc, double rdzc, double2 kx, double2 kxm, double2 ky,
+                                                double2 kym, double2 kz, double2 kzm, double2 kp, double vol) {
+  const double2 g1 = csub(fxp, f), g2 = csub(fxm, f), g3 = csub(fyp, f), g4 = csub(fym, f), g5 = csub(fzp, f),
+                g6 = csub(fzm, f);
+  const double2 Ta = dcfma(rmul(xn5, kxm), g2, cmul(rmul(xn4, kx), g1));
+  const double2 Tb = dcfma(rmul(yn5, kym), g4, cmul(rmul(yn4, ky), g3));
+  const double2 Tc = dcfma(rmul(zn5, kzm), g6, cmul(rmul(zn4, kz), g5));
+  const double2 Ea = dcfma(rmul(rdxc, csub(kx, kxm)), a0m, cmul(rmul(rdxc, csub(kx, kp)), csub(a0, a0m)));
+  const double2 Eb = dcfma(rmul(rdyc, csub(ky, kym)), a1m, cmul(rmul(rdyc, csub(ky, kp)), csub(a1, a1m)));
+  const double2 Ec = dcfma(rmul(rdzc, csub(kz, kzm)), a2m, cmul(rmul(rdzc, csub(kz, kp)), csub(a2, a2m)));
+  const double2 t = cadd(cadd(cadd(Ta, Tb), cadd(Tc, cmul(cmul(kp, kp), f))), cadd(cadd(Ea, Eb), Ec));
+  return rmul(vol, t);
+}
+
+template <bool EPS, bool TIMING>
+__global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __grid_constant__ PassMaps M) {
+  constexpr unsigned kStage = kRawBytes64;
+  extern __shared__ __align__(128) unsigned char shm[];
+  __shared__ int s_item;
+  double2 *Ub = reinterpret_cast<double2 *>(shm + kStages64 * kStage);  // [2][4][kPN]
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * kUBytes64);
+  const bool aligned = (smem_u32(shm) & 127u) == 0;
+  if (!aligned && threadIdx.x == 0) atomicExch(D.err, 2);
+  if (threadIdx.x == 0 && aligned) {
+#pragma unroll
+    for (int q = 0; q < kStages64; q++) mbar_init(smem_u32(&bar[q]));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    fence_async_smem();
+  }
+  unsigned phase = 0;  // bit q: parity of the next wait on stage q
+  const long long per_sys = D.tp.count(), total = aligned ? per_sys * D.nsys : 0;
+
+  for (;;) {
+  __syncthreads();
+  if (threadIdx.x == 0) s_item = atomicAdd(D.work, 1);
+  __syncthreads();
+  const long long item = s_item;
+  if (item >= total) break;
+  const int sys = (int)(item % D.nsys);
+  const long long tile = __ldg(D.order + item / D.nsys);
+  SweepSys *S = D.sys + sys;
+  if (!TIMING && S->phase != PH_INNER) continue;
+
+  const GridDev &g = D.g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  long long tb = tile;
+  const int bi = (int)(tb % D.tp.ti);
+  tb /= D.tp.ti;
+  const int bj = (int)(tb % D.tp.tj);
+  const int bk = (int)(tb / D.tp.tj);
+  const int i0 = bi * kPTI, j0 = bj * kPTJ, k0 = bk * D.tp.kz, k1 = min(nz, k0 + D.tp.kz);
+  const int tx = threadIdx.x % kPTI, ty = threadIdx.x / kPTI;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool live = i < nx && j < ny;
+  const long long N = D.L.N, plane = (long long)D.L.nxp * ny;
+  const long long ndc = i + (long long)D.L.nxp * j;
+  const int cur = S->cur;
+  const long long sb = (long long)sys * 4 * N;
+  double2 *__restrict__ Qw = wvec64(D, cur ^ 1, sys, 0);
+  double2 *__restrict__ Vw = wvec64(D, cur ^ 1, sys, 1);
+  double2 *__restrict__ Pw = wvec64(D, cur ^ 1, sys, 2);
+  double2 *__restrict__ dd = D.dd64 + sb;
+  double2 *__restrict__ xx = D.xx64 + sb;
+  const double *__restrict__ sig = D.sig64;
+  const double *__restrict__ eps = D.epsr64;
+  const double ca = S->vscale;
+  const double2 cb = rmul(-S->vscale, S->beta);
+  const double2 cc = cneg(S->k1);
+  const bool pend = TIMING || S->pending != 0;
+  const double xmix = TIMING ? (double)D.tmix : 1.0;
+  double2 eta = S->eta_pend;
+  double kap = S->kap_pend;
+  if (TIMING) {
+    eta = xmix != 0.0 ? eta : make_double2(0.0, 0.0);
+    kap = xmix != 0.0 ? kap : 1.0;
+  }
+  const double ka = S->ka, kb = S->kb;
+  const int wset = cur * D.nsys + sys;
+
+  // thread 0: the q^ v^ p^ plane m+1 into stage st (x in 8-byte units: even)
+  auto issue = [&](int st, int m) {
+    const unsigned bb = smem_u32(&bar[st]);
+    fence_async_smem();
+    mbar_expect(bb, kStage);
+    tma_load5(smem_u32(shm + st * kStage), &M.w64, 2 * (i0 - 2), j0 - 1, m + 1, 0, wset, bb);
+  };
+  auto wait = [&](int st) {
+    if (!mbar_wait(smem_u32(&bar[st]), (phase >> st) & 1u, kWaitTries) && threadIdx.x == 0) atomicExch(D.err, 1);
+    phase ^= 1u << st;
+  };
+  auto combine = [&](double2 q, double2 v, double2 p, double2 &vo) {
+    vo = dcfma(cb, v, rmul(ca, q));
+    return dcfma(cc, p, vo);
+  };
+  const int eo = (ty + 1) * kPW + (tx + 2);
+  constexpr int kHaloPos = 2 * (kPTI + kPTJ), kHalo = 4 * kHaloPos;
+  auto halo_at = [](int h) {
+    return h < 2 * kPTJ ? (h % kPTJ + 1) * kPW + (h < kPTJ ? 1 : kPTI + 2)
+                        : (h < 2 * kPTJ + kPTI ? 0 : (kPTJ + 1) * kPW) + (h - 2 * kPTJ) % kPTI + 2;
+  };
+
+  double2 um[4], uc[4], up[4], vc[4], vn[4];
+  auto own_step = [&](int st, int m1, double2 *Us, double2 (&uo)[4], double2 (&vo)[4]) {
+    const double2 *R = reinterpret_cast<const double2 *>(shm + st * kStage);
+    const bool owned = live && m1 < k1;
+    const long long nd = ndc + m1 * plane;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      uo[c] = combine(R[c * kPN + eo], R[(4 + c) * kPN + eo], R[(8 + c) * kPN + eo], vo[c]);
+      Us[c * kPN + eo] = uo[c];
+      if (owned) {
+        const long long t = c * N + nd;
+        Vw[t] = vo[c];
+        Pw[t] = uo[c];
+      }
+    }
+  };
+  // lagged update of the own node of plane m1 (p^_{n-1} from stage st; d^, x^
+  // with plain loads)
+  auto dx_step = [&](int st, int m1) {
+    if (live && m1 < k1 && pend) {
+      const double2 *R = reinterpret_cast<const double2 *>(shm + st * kStage);
+      const long long nd = ndc + m1 * plane;
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const long long t = c * N + nd;
+        const double2 d0 = dd[t], x0 = xx[t];
+        const double2 dn = dcfma(eta, R[(8 + c) * kPN + eo], rmul(kap, d0));
+        dd[t] = dn;
+        xx[t] = daxpy(xmix, dn, x0);
+      }
+    }
+  };
+  auto halo = [&](int st, double2 *Us) {
+    const double2 *R = reinterpret_cast<const double2 *>(shm + st * kStage);
+    double2 vt;
+#pragma unroll
+    for (int h = threadIdx.x; h < kHalo; h += kPThreads) {
+      const int hc = h / kHaloPos, he = halo_at(h % kHaloPos);
+      Us[hc * kPN + he] = combine(R[hc * kPN + he], R[(4 + hc) * kPN + he], R[(8 + hc) * kPN + he], vt);
+    }
+  };
+
+  const int ic = min(i, nx - 1), jc = min(j, ny - 1);
+  const double4 *AX = D.ax64, *AY = D.ax64 + 2 * nx, *AZ = D.ax64 + 2 * (nx + ny);
+  const double4 XA = ldg4(AX + ic), XB = ldg4(AX + nx + ic), YA = ldg4(AY + jc), YB = ldg4(AY + ny + jc);
+  const bool hx = live && i < nx - 1, hy = live && j < ny - 1;
+  const bool pxy = live && i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
+  // sigma-bar / eps-bar of component c at node offset q from this column (0
+  // outside the mesh)
+  auto sgl = [&](int c, long long q, bool in) { return in ? __ldg(sig + c * N + q) : 0.0; };
+  auto epl = [&](int c, long long q, bool in) { return !EPS ? 1.0 : (in ? __ldg(eps + c * N + q) : 1.0); };
+
+  if (threadIdx.x == 0) {
+    issue(0, k0 - 1);
+    issue(1, k0);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) um[c] = make_double2(0.0, 0.0);
+  if (live && k0 > 0) {
+    const double2 *Qr = wvec64(D, cur, sys, 0), *Vr = wvec64(D, cur, sys, 1), *Pr = wvec64(D, cur, sys, 2);
+    const long long nd = ndc + (k0 - 1) * plane;
+    double2 vt;
+#pragma unroll
+    for (int c = 0; c < 4; c++) um[c] = combine(__ldg(Qr + c * N + nd), __ldg(Vr + c * N + nd), __ldg(Pr + c * N + nd), vt);
+  }
+  wait(0);
+  own_step(0, k0, Ub, uc, vc);
+  dx_step(0, k0);
+  halo(0, Ub);
+  const long long nd0 = ndc + k0 * plane;
+  double s2m = sgl(2, nd0 - plane, live && k0 > 0);  // sigma-bar of Az at k0-1
+  double e2m = epl(2, nd0 - plane, live && k0 > 0);
+  __syncthreads();
+  if (threadIdx.x == 0 && k0 + 1 <= k1 - 1) issue(0, k0 + 1);
+
+  double acc[kParts];
+#pragma unroll
+  for (int q = 0; q < kParts; q++) acc[q] = 0.0;
+
+  for (int m = k0; m < k1; m++) {
+    const int st = (m - k0 + 1) % kStages64;
+    const double2 *Uc = Ub + ((m - k0) & 1) * 4 * kPN;
+    double2 *Un = Ub + ((m - k0 + 1) & 1) * 4 * kPN;
+    const long long nd = ndc + m * plane;
+    wait(st);
+    own_step(st, m + 1, Un, up, vn);
+    const double4 ZA = ldg4(AZ + m), ZB = ldg4(AZ + nz + m);
+    if (live) {
+      const double sx = sgl(0, nd, true), sy = sgl(1, nd, true), sz = sgl(2, nd, true), sp0 = sgl(3, nd, true);
+      const double spx = sgl(3, nd + 1, i + 1 < nx), spy = sgl(3, nd + D.L.nxp, j + 1 < ny);
+      const double sxm = sgl(0, nd - 1, i > 0), sym = sgl(1, nd - D.L.nxp, j > 0);
+      const double s3p = sgl(3, nd + plane, m + 1 < nz);
+      const double xn4 = XA.x, xn5 = XA.y, dxc = XA.z, rdxc = XA.w, ce2x = XB.x, ce3x = XB.y, dxi = XB.z,
+                   rdxi = XB.w;
+      const double yn4 = YA.x, yn5 = YA.y, dyc = YA.z, rdyc = YA.w, ce2y = YB.x, ce3y = YB.y, dyj = YB.z,
+                   rdyj = YB.w;
+      const double zn4 = ZA.x, zn5 = ZA.y, dzc = ZA.z, rdzc = ZA.w, ce2z = ZB.x, ce3z = ZB.y, dzk = ZB.z,
+                   rdzk = ZB.w;
+      const double2 *U0 = Uc, *U1 = Uc + kPN, *U2 = Uc + 2 * kPN, *U3 = Uc + 3 * kPN;
+      const double2 f0 = uc[3];
+      double2 w0, w1, w2, w3;
+      double ex = 1.0, ey = 1.0, ez = 1.0, ep0 = 1.0, exm = 1.0, eym = 1.0;
+      if (!EPS) {
+        w0 = edge_row64(uc[0], U0[eo + 1], ce2x, U0[eo - 1], ce3x, U0[eo + kPW], yn4, U0[eo - kPW], yn5, up[0], zn4,
+                        um[0], zn5, sx, spx, sp0, U3[eo + 1], f0, rdxi, dxi * dyc * dzc, ka, kb);
+        w1 = edge_row64(uc[1], U1[eo + kPW], ce2y, U1[eo - kPW], ce3y, U1[eo + 1], xn4, U1[eo - 1], xn5, up[1], zn4,
+                        um[1], zn5, sy, spy, sp0, U3[eo + kPW], f0, rdyj, dxc * dyj * dzc, ka, kb);
+        w2 = edge_row64(uc[2], up[2], ce2z, um[2], ce3z, U2[eo + 1], xn4, U2[eo - 1], xn5, U2[eo + kPW], yn4,
+                        U2[eo - kPW], yn5, sz, s3p, sp0, up[3], f0, rdzk, dxc * dyc * dzk, ka, kb);
+        w3 = node_row64(f0, U3[eo + 1], U3[eo - 1], U3[eo + kPW], U3[eo - kPW], up[3], um[3], xn4, xn5, yn4, yn5,
+                        zn4, zn5, uc[0], U0[eo - 1], uc[1], U1[eo - kPW], uc[2], um[2], rdxc, rdyc, rdzc, sx, sxm,
+                        sy, sym, sz, s2m, sp0, dxc * dyc * dzc, ka, kb);
+      } else {
+        ex = epl(0, nd, true), ey = epl(1, nd, true), ez = epl(2, nd, true), ep0 = epl(3, nd, true);
+        exm = epl(0, nd - 1, i > 0), eym = epl(1, nd - D.L.nxp, j > 0);
+        auto K2 = [&](double s_, double e_) { return make_double2(-ka * e_, kb * s_); };
+        const double2 kp0 = K2(sp0, ep0);
+        const double2 kx = K2(sx, ex), ky = K2(sy, ey), kz = K2(sz, ez);
+        w0 = edge_row64_c(uc[0], U0[eo + 1], ce2x, U0[eo - 1], ce3x, U0[eo + kPW], yn4, U0[eo - kPW], yn5, up[0],
+                          zn4, um[0], zn5, kx, K2(spx, epl(3, nd + 1, i + 1 < nx)), kp0, U3[eo + 1], f0, rdxi,
+                          dxi * dyc * dzc);
+        w1 = edge_row64_c(uc[1], U1[eo + kPW], ce2y, U1[eo - kPW], ce3y, U1[eo + 1], xn4, U1[eo - 1], xn5, up[1],
+                          zn4, um[1], zn5, ky, K2(spy, epl(3, nd + D.L.nxp, j + 1 < ny)), kp0, U3[eo + kPW], f0,
+                          rdyj, dxc * dyj * dzc);
+        w2 = edge_row64_c(uc[2], up[2], ce2z, um[2], ce3z, U2[eo + 1], xn4, U2[eo - 1], xn5, U2[eo + kPW], yn4,
+                          U2[eo - kPW], yn5, kz, K2(s3p, epl(3, nd + plane, m + 1 < nz)), kp0, up[3], f0, rdzk,
+                          dxc * dyc * dzk);
+        w3 = node_row64_c(f0, U3[eo + 1], U3[eo - 1], U3[eo + kPW], U3[eo - kPW], up[3], um[3], xn4, xn5, yn4, yn5,
+                          zn4, zn5, uc[0], U0[eo - 1], uc[1], U1[eo - kPW], uc[2], um[2], rdxc, rdyc, rdzc, kx,
+                          K2(sxm, exm), ky, K2(sym, eym), kz, K2(s2m, e2m), kp0, dxc * dyc * dzc);
+      }
+      const double2 zero2 = make_double2(0.0, 0.0);
+      double2 w[4] = {hx ? w0 : zero2, hy ? w1 : zero2, m < nz - 1 ? w2 : zero2,
+                      (pxy && m > 0 && m < nz - 1) ? w3 : zero2};
+      double2 dg[4];
+      const bool pin = pxy && m > 0 && m < nz - 1;
+      jacobi64(XA, XB, YA, YB, ZA, ZB, sx, sy, sz, sp0, pin ? sxm : 0.0, pin ? sym : 0.0, pin ? s2m : 0.0, ex, ey,
+               ez, ep0, pin ? exm : 1.0, pin ? eym : 1.0, pin ? e2m : 1.0, hx, hy, m < nz - 1, pin, ka, kb, dg);
+      double r[kParts];
+#pragma unroll
+      for (int q = 0; q < kParts; q++) r[q] = 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const double2 z = dg[c];
+        double2 d;
+        double rs, mag;
+        jacobi_weights(z, d, rs, mag);
+        const double2 ww = w[c], u = uc[c], v = vc[c];
+        const double2 qh = cmul(d, ww);
+        Qw[c * N + nd] = qh;
+        r[0] += u.x * ww.x - u.y * ww.y;
+        r[1] += u.x * ww.y + u.y * ww.x;
+        r[2] += mag * (ww.x * ww.x + ww.y * ww.y);
+        r[3] += rs * (v.x * qh.x + v.y * qh.y);
+        r[4] += rs * (v.x * qh.y - v.y * qh.x);
+        r[5] += rs * (v.x * v.x + v.y * v.y);
+        r[6] += ww.x * qh.x - ww.y * qh.y;
+        r[7] += ww.x * qh.y + ww.y * qh.x;
+        r[8] += ww.x * v.x - ww.y * v.y;
+        r[9] += ww.x * v.y + ww.y * v.x;
+        const double v2r = v.x * v.x - v.y * v.y, v2i = 2.0 * v.x * v.y;
+        r[10] += v2r * z.x - v2i * z.y;
+        r[11] += v2r * z.y + v2i * z.x;
+      }
+#pragma unroll
+      for (int q = 0; q < kParts; q++) acc[q] += r[q];
+      s2m = sz;
+      e2m = ez;
+    }
+    dx_step(st, m + 1);
+    if (m + 1 < k1) halo(st, Un);
+    __syncthreads();  // everyone is done with stage st and with u plane m
+    if (threadIdx.x == 0 && m + 2 <= k1 - 1) issue(st, m + 2);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      um[c] = uc[c];
+      uc[c] = up[c];
+      vc[c] = vn[c];
+    }
+  }
+
+  Vals<kParts> blk;
+#pragma unroll
+  for (int q = 0; q < kParts; q++) blk.v[q] = acc[q];
+  blk = block_reduce<kParts, kPThreads>(blk);
+  double *part = D.part + (size_t)sys * D.slots * kParts;
+  unsigned *cnt = D.cnt + CNT_PASS * D.nsys + sys;
+  const unsigned nt = (unsigned)D.tp.count();
+  if (arrive<kParts, kPThreads>(blk, part, cnt, (unsigned)tile, nt)) {
+    Vals<kParts> tot = final_reduce<kParts, kPThreads>(part, cnt, nt);
+    if (threadIdx.x == 0) {
+      if (TIMING)
+        S->cur ^= 1;
+      else
+        pass_scalars(S, tot.v);
+    }
+  }
+  }  // work items
   if (threadIdx.x == 0) {
     __threadfence();
     if (atomicAdd(D.work + 1, 1) == gridDim.x - 1) {

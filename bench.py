@@ -124,6 +124,8 @@ def run_reference(args):
     if rank != 0:
         return 0
     iters = FP64_ITERS.get(args.workload)
+    from aphid_git_b200 import model
+    m = model.make_model(args.workload)
     sample_it = args.cpu_sample_iters
     times = []
     for step in range(args.warmup + args.steps):
@@ -137,7 +139,9 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": spi * iters * 1e3 if iters else None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.workload, "target": TARGET},
+        "config": {"workload": args.workload, "precision": "complex128 (the reference's algorithm, CPU)",
+                   "unknowns": int(m.n), "systems": len(systems_of(m)[0]), "target": TARGET,
+                   "parallelism": "one process, 4 threads (qmr_mthread component split)"},
         "s_per_iter": spi, "iters_to_tol": iters,
         "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": 4, "kind": "port",
                          "sample": "%d QMR iterations per step, 4-thread component split; "

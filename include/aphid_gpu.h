@@ -60,6 +60,10 @@ typedef struct aphid_ctx aphid_ctx;
 /* precision of aphid_gpu_sweep */
 #define APHID_PREC_FP64      0   /* plain complex128 Jacobi-QMR, the reference's algorithm */
 #define APHID_PREC_MIXED     1   /* complex64 inner QMR inside FP64 defect correction */
+#define APHID_PREC_FUSED64   2   /* complex128 inner QMR, the batched fused pass in FP64 */
+#define APHID_PREC_AUTO      3   /* MIXED; a system whose complex-symmetric Lanczos form
+                                    v^T v collapses below complex64 resolution is finished
+                                    by FUSED64 from its current iterate */
 
 typedef struct {
   int device;        /* CUDA device ordinal */
@@ -82,6 +86,8 @@ typedef struct {
   double true_rel_resid;    /* ||b - K x||_2 / ||b||_2 recomputed in FP64 */
   double seconds;           /* device time of the solve (CUDA events) */
   long long kernel_launches; /* kernels this call launched (graph nodes included) */
+  int inner64_iters;        /* of inner_iters, those run in complex128 (FUSED64, or
+                               AUTO after escalation) */
 } aphid_info;
 
 /* ---- context --------------------------------------------------------- */
@@ -194,17 +200,22 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re,
                         const float *eps_rel);
 
 typedef struct {
-  int precision;      /* APHID_PREC_MIXED or APHID_PREC_FP64 */
-  double target;      /* MIXED: stop when ||b - K x||_2 < target ||b||_2 (FP64
-                         true residual); FP64: the reference's recurrence
-                         stop test with this qmr_target */
+  int precision;      /* APHID_PREC_FP64, _MIXED, _FUSED64 or _AUTO */
+  double target;      /* MIXED, FUSED64, AUTO: stop when ||b - K x||_2 <
+                         target ||b||_2 (FP64 true residual); FP64: the
+                         reference's recurrence stop test with this
+                         qmr_target */
   int max_it;         /* iteration cap per system (inner iterations, MIXED) */
   double inner_tol;   /* MIXED: cap on the inner quasi-residual reduction per
                          defect-correction step (0 = 1e-10); a cycle also
                          ends when the true residual, checked every graph
                          round, converges or stagnates */
   int max_outer;      /* MIXED: cap on defect-correction steps (0 = 40) */
-  int reserved[3];
+  int stall_window;   /* MIXED, AUTO: a cycle whose quasi-residual has not
+                         halved over this many inner iterations restarts from
+                         the FP64 residual (0 = 400, < 0 = never); FUSED64:
+                         0 = never */
+  int reserved[2];
 } aphid_sweep_opts;
 
 /* Solve nsys systems (frequency x source) on the context's mesh and model:
@@ -232,13 +243,24 @@ int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx);
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);
 
 /* Benchmarking hook, no counterpart in the reference: launch the fused
- * complex64 QMR iteration pass (p update, q^ = D^-1 K p^, the lagged d/x
+ * QMR iteration pass (complex64, or complex128 after a FUSED64 sweep) (p update, q^ = D^-1 K p^, the lagged d/x
  * update with zero weights, the inner products) `reps` times over all
  * systems of the last mixed-precision sweep, on the context's stream, without
  * the scalar recurrence.  The solutions (aphid_gpu_sweep_fetch) are not
  * changed; the inner Krylov vectors are, as by an iteration.  Returns after
  * the launches (asynchronous). */
 int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps);
+
+/* Testing hook, no counterpart in the reference: y = K x with the operator of
+ * the fused pass of the last batched sweep -- the complex64 pass (x rounded
+ * to complex64, the rows in FP32 arithmetic) after MIXED or AUTO, the
+ * complex128 pass after FUSED64 -- for its system 0 (that frequency, on the
+ * context's model), so that tests can hold each pass to the reference's K
+ * (src/aphid_qmr.f90 inprod_*) row by row.  x and y are host arrays of n
+ * complex128.  Like aphid_gpu_sweep_time_apply it overwrites the inner
+ * Krylov vectors of that sweep; the solutions are kept.  Synchronises the
+ * stream. */
+int aphid_gpu_sweep_apply(aphid_ctx *ctx, const aphid_z *x, aphid_z *y);
 
 /* ---- allocation-free operator apply -------------------------------------- */
 

@@ -78,18 +78,20 @@ def test_sweep_fp64_matches_oracle(solver):
 
 
 @pytest.mark.parametrize("mode", ["R", "C", "I"])
-def test_sweep_mixed_fields_within_1e6(solver, mode):
+@pytest.mark.parametrize("precision", ["mixed", "fused64"])
+def test_sweep_mixed_fields_within_1e6(solver, mode, precision):
     xn, yn, zn, sig, epsr = small_model(seed=5)
     solver.set_nodes(xn, yn, zn)
     solver.set_model(mode, sig if mode != "I" else None, epsr if mode != "R" else None)
     freqs = [1e-2, 1.0, 1e2, 1e4] if mode != "I" else [1e6, 1e7, 1e8]
     src = [[("+X", 6, 6, 4)]]
     om = [2 * np.pi * f for f in freqs]
-    X, infos = solver.sweep(om, src, [0] * len(om), precision="mixed", target=1e-8, max_it=20000)
+    X, infos = solver.sweep(om, src, [0] * len(om), precision=precision, target=1e-8, max_it=20000)
     for s, w in enumerate(om):
         info = infos[s]
         assert info["status_name"] == "converged", info
         assert info["true_rel_resid"] < 1e-8
+        assert info["inner64_iters"] == (info["inner_iters"] if precision == "fused64" else 0)
         g, k2, b, ref = oracle_solve(xn, yn, zn, mode, w, sig.ravel(order="F"),
                                      epsr.ravel(order="F"), src[0])
         # the device residual is the true one: recompute it with the oracle's operator
@@ -195,3 +197,74 @@ def test_autotuner_picks_and_caches_the_slab_depth(tmp_path, monkeypatch):
     for a, b, ia, ib in zip(X1, X3, i1, i3):
         assert ia["status_name"] == ib["status_name"] == "converged"
         assert relerr(a, b) < 1e-6
+
+
+@pytest.mark.parametrize("precision,tol_norm,tol_row", [("mixed", 1e-6, 1e-5), ("fused64", 1e-13, 1e-11)])
+@pytest.mark.parametrize("mode", ["R", "C"])
+def test_pass_operator_matches_oracle_row_by_row(solver, mode, precision, tol_norm, tol_row):
+    """The operator each fused pass applies, y = K x, against the reference's
+    K (oracle inprod, complex128) on a random vector, row by row: within the
+    rounding of complex64 inputs and FP32 arithmetic for the complex64 pass,
+    within FP64 rounding for the complex128 pass."""
+    xn, yn, zn, sig, epsr = small_model(seed=11, dims=(22, 19, 21), nair=4)
+    sig[:, :, 4:7] = 3.3  # a conductive layer under the air: the hardest contrast
+    w = 2 * np.pi * 0.3
+    solver.set_nodes(xn, yn, zn)
+    solver.set_model(mode, sig, None if mode == "R" else epsr)
+    solver.sweep([w], [[("+X", 10, 10, 5)]], [0], max_it=2, precision=precision, fetch=False)
+    g = O.Grid(xn, yn, zn)
+    k2 = O.gen_k2(g, O.sigma_hat(mode, w, sig_re=sig, eps_rel=None if mode == "R" else epsr), w)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(g.n) + 1j * rng.standard_normal(g.n)
+    y = solver.sweep_apply(x)
+    y64 = O.inprod(g, k2, x)
+    floor = 1e-3 * np.sqrt(np.mean(np.abs(y64) ** 2))
+    assert relerr(y, y64) < tol_norm
+    assert np.max(np.abs(y - y64) / (np.abs(y64) + floor)) < tol_row
+
+
+def sea_model(nc, seed=6):
+    """nc^3 cells, 10 air layers over 15 layers of seawater (3.3 S/m) over a
+    heterogeneous earth, +X dipole on the sea floor: complex-symmetric
+    Lanczos loses its bilinear form here below complex64 resolution."""
+    nair, nsea = 10, 15
+    rng = np.random.default_rng(seed)
+    xn, yn = model.graded_axis(nc), model.graded_axis(nc)
+    zn = model.depth_axis(nc, nair)
+    sig = model._earth((nc, nc, nc), nair + nsea, rng)
+    sig[:, :, nair:nair + nsea] = 3.3
+    return xn, yn, zn, sig.astype(np.float32), [[("+X", nc // 2, (nc + 2) // 2, nair + nsea + 1)]]
+
+
+def test_auto_escalates_seafloor_and_keeps_land_in_complex64(solver):
+    """AUTO on a seafloor model at 0.27 Hz, where the complex64 inner solve
+    needs several times the complex128 iterations: the system is escalated
+    to the complex128 pass and finishes within 15% of the reference
+    algorithm's iteration count.  On a land model nothing escalates and AUTO
+    is MIXED."""
+    xn, yn, zn, sig, src = sea_model(96)
+    solver.set_nodes(xn, yn, zn)
+    solver.set_model("R", sig)
+    w = [2 * np.pi * 0.272, 2 * np.pi * 1.35]
+    _, ref = solver.sweep(w, src, [0, 0], precision="fp64", fetch=False)
+    X, auto = solver.sweep(w, src, [0, 0], precision="auto")
+    _, mixed = solver.sweep(w, src, [0, 0], precision="mixed", fetch=False)
+    for s in range(2):
+        assert auto[s]["status_name"] == "converged" and auto[s]["true_rel_resid"] < 1e-8
+        assert auto[s]["inner64_iters"] > 0
+        assert auto[s]["inner_iters"] <= 1.15 * ref[s]["iters"]
+    assert mixed[0]["inner_iters"] > 2 * ref[0]["iters"]
+    # the answer is the system's: the oracle's operator gives the same residual
+    g = O.Grid(xn, yn, zn)
+    k2 = O.gen_k2(g, O.sigma_hat("R", w[0], sig_re=sig.ravel(order="F")), w[0])
+    b, _ = O.gen_rhs(g, 5, src[0])
+    assert np.linalg.norm(b - O.inprod(g, k2, X[0])) / np.linalg.norm(b) < 2e-8
+    # land: no escalation, bit-identical to MIXED
+    xn, yn, zn, sig, _ = small_model(seed=5, dims=(40, 40, 40), nair=8)
+    solver.set_nodes(xn, yn, zn)
+    solver.set_model("R", sig)
+    src = [[("+X", 20, 20, 9)]]
+    Xa, ia = solver.sweep([2 * np.pi], src, [0], precision="auto")
+    Xm, im = solver.sweep([2 * np.pi], src, [0], precision="mixed")
+    assert ia[0]["inner64_iters"] == 0 and ia[0]["inner_iters"] == im[0]["inner_iters"]
+    assert np.array_equal(Xa, Xm)
