@@ -227,7 +227,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hetero96")
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "auto", "fused64", "fp64"])
+    ap.add_argument("--plain-sweep", action="store_true",
+                    help="also time the plain complex128 path over every system of the workload "
+                         "(one solve each, the reference's algorithm) and report the ratio")
     ap.add_argument("--inner-tol", type=float, default=0.0)
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="timed complex128 solves for the speed-up comparison (0: skip)")
@@ -339,7 +342,7 @@ def main():
         s.set_model("R", m.sig_re)
 
         def run_sweep():
-            return s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=MAX_IT,
+            return s.sweep(om, m.sources, sos, precision=args.precision, target=TARGET, max_it=MAX_IT,
                            inner_tol=args.inner_tol, fetch=False)[1]
 
         for _ in range(args.warmup):
@@ -354,7 +357,7 @@ def main():
 
         def run_e2e():
             s.set_model("R", m.sig_re)
-            return s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=MAX_IT,
+            return s.sweep(om, m.sources, sos, precision=args.precision, target=TARGET, max_it=MAX_IT,
                            inner_tol=args.inner_tol, fetch=True)[1]
 
         ms_e, _ = timed(stream, dev, run_e2e, args.steps, barrier, world)
@@ -363,24 +366,43 @@ def main():
         # dominant kernel: the fused complex64 QMR iteration (one launch per
         # inner iteration); algorithmic bytes per launch in pass_bytes().
         reps = 20
+        if args.precision == "auto":
+            # escalation releases the complex64 state: rebuild it for the timing launches
+            s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=8, fetch=False)
         s.sweep_time_apply(3)
         ms_a, _ = timed(stream, dev, lambda: s.sweep_time_apply(reps), 1, lambda: None, 1)
         t_apply = ms_a * 1e-3 / reps
-        alg = pass_bytes(nsys, n)
-        kernel = ("k_sw_pass (fused complex64 QMR iteration: p^ update, q^ = D^-1 K p^, "
-                  "lagged d^/x^ update, 12 inner products)")
+        f64 = args.precision == "fused64"
+        alg = pass_bytes(nsys, n) * (2 if f64 else 1)
+        kernel = ("k_sw_pass64 (fused complex128 QMR iteration" if f64 else
+                  "k_sw_pass (fused complex64 QMR iteration") + (
+                  ": p^ update, q^ = D^-1 K p^, lagged d^/x^ update, 12 inner products)")
         it_in = [i["inner_iters"] for i in last]
         extra = {"time_to_tol_s": ms / args.steps * 1e-3, "systems": nsys,
                  "inner_iters_max": max(it_in), "inner_iters_total": int(sum(it_in)),
                  "outer_iters_max": max(i["outer_iters"] for i in last),
                  "qmr_iters_per_s": world * args.steps * sum(it_in) / (ms * 1e-3),
+                 "inner64_iters_total": int(sum(i["inner64_iters"] for i in last)),
                  "true_rel_resid_max": max(i["true_rel_resid"] for i in last),
                  "status": sorted({i["status_name"] for i in last})}
+        if args.plain_sweep:
+            # the plain complex128 path over every system, once
+            ms_p, inf_p = timed(stream, dev, lambda: s.sweep(om, m.sources, sos, precision="fp64", target=TARGET,
+                                                              max_it=MAX_IT, fetch=False)[1], 1, barrier, world)
+            pi = inf_p[-1]
+            extra["plain_fp64_sweep"] = {
+                "time_s": ms_p * 1e-3, "iters": [i["iters"] for i in pi],
+                "status": sorted({i["status_name"] for i in pi}),
+                "note": "complex128 Jacobi-QMR, the reference's recurrence and stop test, one system "
+                        "at a time on the same GPU"}
+            extra["speedup_vs_plain_fp64_sweep"] = ms_p * 1e-3 / (ms / args.steps * 1e-3)
+            extra["inner_iters"] = it_in
         if plain is not None:
             extra["plain_fp64"] = plain
             extra["speedup_vs_plain_fp64"] = plain["time_to_tol_s"] * nsys / (ms / args.steps * 1e-3)
-        dtype = "c64 inner / f64 outer"
-        traffic_key = "sw_pass_" + args.workload
+        dtype = {"mixed": "c64 inner / f64 outer", "fused64": "c128 inner / f64 outer",
+                 "auto": "c64 inner (c128 after escalation) / f64 outer"}[args.precision]
+        traffic_key = ("sw_pass64_" if f64 else "sw_pass_") + args.workload
 
     achieved = alg / t_apply / 1e9
     traffic = None
