@@ -270,16 +270,16 @@ __device__ __forceinline__ void jacobi64(double4 XA, double4 XB, double4 YA, dou
   }
 }
 __device__ __forceinline__ void jacobi_weights(double2 z, double2 &inv, double &absd, double &rabsd) {
-  const double mz = fmax(fabs(z.x), fabs(z.y));
+  // |z|^2 stays far inside the FP64 range here, so no pre-scaling: one
+  // reciprocal square root gives D^-1 = conj(z) / |z|^2, |D| and 1/|D|
+  const double n2 = __dadd_rn(__dmul_rn(z.x, z.x), __dmul_rn(z.y, z.y));
   inv = make_double2(0.0, 0.0);
   absd = rabsd = 0.0;
-  if (mz > 0.0) {
-    const double sc = __ddiv_rn(1.0, mz), za = __dmul_rn(z.x, sc), zb = __dmul_rn(z.y, sc);
-    const double n2 = __dadd_rn(__dmul_rn(za, za), __dmul_rn(zb, zb)), rn = __ddiv_rn(1.0, __dsqrt_rn(n2));
-    const double t = __dmul_rn(sc, __dmul_rn(rn, rn));
-    inv = make_double2(__dmul_rn(za, t), -__dmul_rn(zb, t));
-    absd = __dmul_rn(__dmul_rn(mz, n2), rn);
-    rabsd = __dmul_rn(sc, rn);
+  if (n2 > 0.0) {
+    const double rn = rsqrt(n2), t = __dmul_rn(rn, rn);
+    inv = make_double2(__dmul_rn(z.x, t), -__dmul_rn(z.y, t));
+    absd = __dmul_rn(n2, rn);
+    rabsd = rn;
   }
 }
 
@@ -1404,6 +1404,9 @@ constexpr unsigned kRawBytes64 = 12u * kPN * 16u;  // q^, v^, p^ with halo, four
 constexpr unsigned kUBytes64 = 4u * kPN * 16u;
 constexpr size_t kPass64Shm = kStages64 * (size_t)kRawBytes64 + 2 * (size_t)kUBytes64 + 128;
 
+// pull a line towards this SM's L1 ahead of its use (no register, no wait)
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ double2 daxpy(double a, double2 x, double2 y) {
   return make_double2(fma(a, x.x, y.x), fma(a, x.y, y.y));
 }
@@ -1642,6 +1645,29 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
     const double2 *Uc = Ub + ((m - k0) & 1) * 4 * kPN;
     double2 *Un = Ub + ((m - k0 + 1) & 1) * 4 * kPN;
     const long long nd = ndc + m * plane;
+    if (live) {
+      // the plain loads of the next plane (sigma-bar) and of the lagged
+      // update one plane further (d^, x^) start now, under this plane's work
+      if (m + 1 < k1) {
+        const long long n1 = nd + plane;
+#pragma unroll
+        for (int c = 0; c < 4; c++) prefetch_l1(sig + c * N + n1);
+        if (j + 1 < ny) prefetch_l1(sig + 3 * N + n1 + D.L.nxp);
+        if (j > 0) prefetch_l1(sig + N + n1 - D.L.nxp);
+        if (EPS) {
+#pragma unroll
+          for (int c = 0; c < 4; c++) prefetch_l1(eps + c * N + n1);
+        }
+      }
+      if (pend && m + 2 < k1) {
+        const long long n2 = nd + 2 * plane;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          prefetch_l1(dd + c * N + n2);
+          prefetch_l1(xx + c * N + n2);
+        }
+      }
+    }
     wait(st);
     own_step(st, m + 1, Un, up, vn);
     const double4 ZA = ldg4(AZ + m), ZB = ldg4(AZ + nz + m);
@@ -1765,5 +1791,6 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
     }
   }
 }
+
 
 }  // namespace aphid
