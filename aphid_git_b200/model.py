@@ -382,6 +382,8 @@ def make_model(config, seed=None):
     seafloor256   256x256x192 cells, 10 air layers, 15 seawater layers at
                   3.3 S/m, heterogeneous earth, 24 frequencies, one +X dipole
                   on the seafloor
+    seafloor96    the same layering on 96^3 cells at 0.272 Hz, where the
+                  complex64 Lanczos form collapses (escalation test case)
     """
     cfg = {
         "halfspace32": (32, 32, 32, 8, 0, 1),
@@ -390,6 +392,7 @@ def make_model(config, seed=None):
         "train64": (64, 64, 48, 8, 0, 4),
         "eval160": (160, 160, 128, 8, 0, 5),
         "seafloor256": (256, 256, 192, 10, 15, 6),
+        "seafloor96": (96, 96, 96, 10, 15, 6),
     }
     if config not in cfg:
         raise KeyError("unknown synthetic model %r" % config)
@@ -414,6 +417,9 @@ def make_model(config, seed=None):
     elif config == "seafloor256":
         sources = [[("+X", ic, jc, ks)]]
         freqs = np.logspace(-3, 5, 24)
+    elif config == "seafloor96":
+        sources = [[("+X", ic, jc, ks)]]
+        freqs = [0.272]
     else:
         sources = [[("+X", ic, jc, ks)]]
         freqs = [1.0]

@@ -280,10 +280,12 @@ def main():
     if args.one_sweep:
         # one mixed sweep of the workload, nothing timed (profiling target)
         s.set_model("R", m.sig_re)
-        _, inf = s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=MAX_IT, fetch=False)
-        print(json.dumps({"workload": args.workload, "systems": nsys, "plane_kz": s.sweep_plane_kz(),
+        prec = "mixed" if args.precision == "fp64" else args.precision
+        _, inf = s.sweep(om, m.sources, sos, precision=prec, target=TARGET, max_it=MAX_IT, fetch=False)
+        print(json.dumps({"workload": args.workload, "precision": prec, "systems": nsys, "plane_kz": s.sweep_plane_kz(),
                           "inner_iters": [i["inner_iters"] for i in inf][:8],
                           "outer_iters": [i["outer_iters"] for i in inf][:8],
+                          "inner64_iters": [i["inner64_iters"] for i in inf][:8],
                           "seconds": inf[0]["seconds"], "launches": inf[0]["kernel_launches"]}))
         return 0
 
