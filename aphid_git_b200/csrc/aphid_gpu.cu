@@ -762,7 +762,20 @@ int vector_maps64(aphid_ctx *ctx) {
   const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * 16, (cuuint64_t)L.nxp * ctx->ny * 16, (cuuint64_t)L.N * 16,
                                  (cuuint64_t)L.N * 192};
   const cuuint32_t box[5] = {2 * kPW, kPH, 1, 12, 1};
-  return encode_map(ctx, &ctx->maps.w64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64, dims, strides, box);
+  int rc = encode_map(ctx, &ctx->maps.w64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64, dims, strides, box);
+  if (rc) return rc;
+  // d^, x^: (2 nxp, ny, nz, component, system); one box = the 16 x 16 tile
+  const size_t v64 = (size_t)ctx->sw_nsys64 * 4 * L.N;
+  const cuuint64_t odims[5] = {2 * (cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4,
+                               (cuuint64_t)ctx->sw_nsys64};
+  const cuuint64_t ostrides[4] = {(cuuint64_t)L.nxp * 16, (cuuint64_t)L.nxp * ctx->ny * 16, (cuuint64_t)L.N * 16,
+                                  (cuuint64_t)L.N * 64};
+  const cuuint32_t obox[5] = {2 * kPTI, kPTJ, 1, 4, 1};
+  if ((rc = encode_map(ctx, &ctx->maps.dd64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64 + 6 * v64, odims, ostrides,
+                       obox)))
+    return rc;
+  return encode_map(ctx, &ctx->maps.xx64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64 + 7 * v64, odims, ostrides,
+                    obox);
 }
 
 // sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18

@@ -877,6 +877,7 @@ struct PassMaps {
   CUtensorMap sig, eps;  // 4-D: (nxp, ny, nz, component), FP32
   CUtensorMap dd, xx;    // 5-D: (nxp, ny, nz, component, system), 8-byte elements
   CUtensorMap w64;       // complex128 q^ v^ p^: 5-D (2 nxp, ny, nz, 12, set x system), 8-byte elements
+  CUtensorMap dd64, xx64;  // complex128 d^, x^: 5-D (2 nxp, ny, nz, component, system), 8-byte elements
 };
 
 constexpr int kStages = 3;                       // load ring depth of the pass
@@ -1397,12 +1398,14 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
 // FP64 coefficients (sigma-bar, eps-bar, axis tables) and FP64 arithmetic, for
 // systems on which complex64 storage cannot carry the Lanczos process (see
 // kDeltaFloor).  Same tiles, same work order, same inner products and scalar
-// step (pass_scalars); 2 TMA stages of q^ v^ p^ planes (69 KB each); sigma-bar
-// and d^, x^ are read with plain loads.
+// step (pass_scalars); 2 TMA stages of q^ v^ p^ planes (69 KB each) and one
+// TMA buffer of the own tile's d^, x^ (32 KB), loaded a plane ahead;
+// sigma-bar is read with plain loads, prefetched into L1 a plane ahead.
 constexpr int kStages64 = 2;
 constexpr unsigned kRawBytes64 = 12u * kPN * 16u;  // q^, v^, p^ with halo, four components, complex128
 constexpr unsigned kUBytes64 = 4u * kPN * 16u;
-constexpr size_t kPass64Shm = kStages64 * (size_t)kRawBytes64 + 2 * (size_t)kUBytes64 + 128;
+constexpr unsigned kDXBytes64 = 2u * 4u * kPThreads * 16u;  // d^ and x^ of one plane of the own tile
+constexpr size_t kPass64Shm = kStages64 * (size_t)kRawBytes64 + 2 * (size_t)kUBytes64 + kDXBytes64 + 128;
 
 // pull a line towards this SM's L1 ahead of its use (no register, no wait)
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
@@ -1480,16 +1483,19 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
   double2 *Ub = reinterpret_cast<double2 *>(shm + kStages64 * kStage);  // [2][4][kPN]
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * kUBytes64);
+  // d^ then x^ of the own tile, one plane, [4][kPThreads] each
+  const double2 *DX = reinterpret_cast<const double2 *>(shm + kStages64 * kStage + 2 * kUBytes64);
+  unsigned long long *bar =
+      reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * kUBytes64 + kDXBytes64);
   const bool aligned = (smem_u32(shm) & 127u) == 0;
   if (!aligned && threadIdx.x == 0) atomicExch(D.err, 2);
   if (threadIdx.x == 0 && aligned) {
 #pragma unroll
-    for (int q = 0; q < kStages64; q++) mbar_init(smem_u32(&bar[q]));
+    for (int q = 0; q <= kStages64; q++) mbar_init(smem_u32(&bar[q]));  // the ring, then the d^/x^ buffer
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     fence_async_smem();
   }
-  unsigned phase = 0;  // bit q: parity of the next wait on stage q
+  unsigned phase = 0;  // bit q: parity of the next wait on stage q (bit kStages64: d^/x^)
   const long long per_sys = D.tp.count(), total = aligned ? per_sys * D.nsys : 0;
 
   for (;;) {
@@ -1550,6 +1556,15 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
     if (!mbar_wait(smem_u32(&bar[st]), (phase >> st) & 1u, kWaitTries) && threadIdx.x == 0) atomicExch(D.err, 1);
     phase ^= 1u << st;
   };
+  // thread 0: d^ and x^ of plane m1's own tile (x origin 2 i0: even)
+  auto issue_dx = [&](int m1) {
+    const unsigned bb = smem_u32(&bar[kStages64]);
+    unsigned char *base = shm + kStages64 * kStage + 2 * kUBytes64;
+    fence_async_smem();
+    mbar_expect(bb, kDXBytes64);
+    tma_load5(smem_u32(base), &M.dd64, 2 * i0, j0, m1, 0, sys, bb);
+    tma_load5(smem_u32(base + kDXBytes64 / 2), &M.xx64, 2 * i0, j0, m1, 0, sys, bb);
+  };
   auto combine = [&](double2 q, double2 v, double2 p, double2 &vo) {
     vo = dcfma(cb, v, rmul(ca, q));
     return dcfma(cc, p, vo);
@@ -1580,13 +1595,14 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   // lagged update of the own node of plane m1 (p^_{n-1} from stage st; d^, x^
   // with plain loads)
   auto dx_step = [&](int st, int m1) {
+    if (m1 < k1 && pend) wait(kStages64);
     if (live && m1 < k1 && pend) {
       const double2 *R = reinterpret_cast<const double2 *>(shm + st * kStage);
       const long long nd = ndc + m1 * plane;
 #pragma unroll
       for (int c = 0; c < 4; c++) {
         const long long t = c * N + nd;
-        const double2 d0 = dd[t], x0 = xx[t];
+        const double2 d0 = DX[c * kPThreads + threadIdx.x], x0 = DX[(4 + c) * kPThreads + threadIdx.x];
         const double2 dn = dcfma(eta, R[(8 + c) * kPN + eo], rmul(kap, d0));
         dd[t] = dn;
         xx[t] = daxpy(xmix, dn, x0);
@@ -1616,6 +1632,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   if (threadIdx.x == 0) {
     issue(0, k0 - 1);
     issue(1, k0);
+    if (pend) issue_dx(k0);
   }
 #pragma unroll
   for (int c = 0; c < 4; c++) um[c] = make_double2(0.0, 0.0);
@@ -1635,6 +1652,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   double e2m = epl(2, nd0 - plane, live && k0 > 0);
   __syncthreads();
   if (threadIdx.x == 0 && k0 + 1 <= k1 - 1) issue(0, k0 + 1);
+  if (threadIdx.x == 0 && pend && k0 + 1 < k1) issue_dx(k0 + 1);
 
   double acc[kParts];
 #pragma unroll
@@ -1657,14 +1675,6 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
         if (EPS) {
 #pragma unroll
           for (int c = 0; c < 4; c++) prefetch_l1(eps + c * N + n1);
-        }
-      }
-      if (pend && m + 2 < k1) {
-        const long long n2 = nd + 2 * plane;
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-          prefetch_l1(dd + c * N + n2);
-          prefetch_l1(xx + c * N + n2);
         }
       }
     }
@@ -1755,8 +1765,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
     }
     dx_step(st, m + 1);
     if (m + 1 < k1) halo(st, Un);
-    __syncthreads();  // everyone is done with stage st and with u plane m
+    __syncthreads();  // everyone is done with stage st, u plane m and the d^/x^ buffer
     if (threadIdx.x == 0 && m + 2 <= k1 - 1) issue(st, m + 2);
+    if (threadIdx.x == 0 && pend && m + 2 < k1) issue_dx(m + 2);
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       um[c] = uc[c];
