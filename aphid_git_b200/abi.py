@@ -280,12 +280,20 @@ class Solver:
             self._model[0].ctypes.data if self._model[0] is not None else None,
             self._model[1].ctypes.data if self._model[1] is not None else None), "set_model")
 
-    def sweep(self, omegas, sources, source_of_system=None, x0=None, precision="mixed",
-              target=1e-8, max_it=20000, inner_tol=0.0, max_outer=0, stall_window=0, fetch=True):
+    def sweep(self, omegas, sources, source_of_system=None, x0=None, precision="auto",
+              target=1e-8, max_it=20000, inner_tol=0.0, max_outer=0, stall_window=0, fetch=True,
+              out=None):
         """Solve all (omega, source) systems in one batched launch.
 
         sources: list of oper_mode-5 dipole lists [(dir, i, j, k), ...];
         source_of_system[s] picks the source of system s (default: s).
+        precision: "auto" (complex64 inner solves; systems whose Lanczos
+        bilinear form collapses below complex64 resolution finish in
+        complex128), "mixed", "fused64" (complex128 inner solves, same
+        batched pass) or "fp64" (the reference's recurrence, one system at a
+        time).
+        out: an optional C-contiguous complex128 (nsys, nunk) array (pinned
+        host memory makes the copy fastest) that receives the solutions.
         Returns (X, infos): X is (nsys, nunk) complex128 (None when fetch is
         False: the solutions stay on the device, see sweep_fetch)."""
         om = np.ascontiguousarray(np.atleast_1d(omegas), dtype=np.float64)
@@ -297,7 +305,12 @@ class Solver:
         ijk = np.array([[int(d[1]), int(d[2]), int(d[3])] for q in sources for d in q] or
                        [[0, 0, 0]], dtype=np.int32)
         x0a = None if x0 is None else np.ascontiguousarray(x0, dtype=np.complex128).reshape(nsys, self.n)
-        X = np.empty((nsys, self.n), np.complex128) if fetch else None
+        if out is not None:
+            if (out.dtype != np.complex128 or out.shape != (nsys, self.n) or not out.flags["C_CONTIGUOUS"]):
+                raise AphidError("out must be a C-contiguous complex128 array of shape (%d, %d)" % (nsys, self.n))
+            X = out
+        else:
+            X = np.empty((nsys, self.n), np.complex128) if fetch else None
         infos = (Info * nsys)()
         if precision not in PRECISIONS:
             raise AphidError("precision must be one of %s" % ", ".join(PRECISIONS))

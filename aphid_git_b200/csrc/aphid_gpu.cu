@@ -69,6 +69,8 @@ struct aphid_ctx {
   double *d_sig = nullptr, *d_epsr = nullptr;
   float *d_sig32 = nullptr, *d_epsr32 = nullptr;
   double *d_sig64 = nullptr, *d_epsr64 = nullptr;  // FP64 node-layout copies (complex128 pass)
+  float *d_cells = nullptr;  // staging of the real(4) cell arrays (set_model)
+  long long cells_cap = 0;
   // sweep state
   int sw_nsys = 0;           // systems the buffers hold
   bool sw_f32_ok = false;    // complex64 vectors allocated
@@ -322,6 +324,7 @@ int aphid_gpu_destroy(aphid_ctx *ctx) {
   cudaFree(ctx->d_epsr32);
   cudaFree(ctx->d_sig64);
   cudaFree(ctx->d_epsr64);
+  cudaFree(ctx->d_cells);
   if (ctx->h_done) cudaFreeHost(ctx->h_done);
   if (ctx->h_ndone) cudaFreeHost(ctx->h_ndone);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -1409,8 +1412,14 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
     ctx->d_epsr32 = nullptr;
     ctx->d_epsr64 = nullptr;
   }
-  float *cells = nullptr;
-  CK(cudaMalloc(&cells, ncell * sizeof(float)));
+  if (ctx->cells_cap < ncell) {
+    cudaFree(ctx->d_cells);
+    ctx->d_cells = nullptr;
+    ctx->cells_cap = 0;
+    CK(cudaMalloc(&ctx->d_cells, ncell * sizeof(float)));
+    ctx->cells_cap = ncell;
+  }
+  float *cells = ctx->d_cells;
   const dim3 grid = node_grid(ctx);
   if (csig_flag == 'I') {
     CK(cudaMemsetAsync(ctx->d_sig, 0, ctx->n * sizeof(double), ctx->stream));
@@ -1432,7 +1441,6 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
   k_sw_to_node<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_sig, ctx->d_sig64);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
-  cudaFree(cells);
   if ((rc = model_maps(ctx))) return rc;
   ctx->csig = csig_flag;
   ctx->has_model = true;
