@@ -27,6 +27,7 @@
         type(c_ptr)    :: stream
         integer(c_int) :: graph_iters
         integer(c_int) :: verbose
+        integer(c_int) :: plane_kz
       end type aphid_opts
 
       type, bind(C) :: aphid_info
@@ -34,6 +35,7 @@
         real(c_double)       :: rhs_norm, recur_resid, true_rel_resid
         real(c_double)       :: seconds
         integer(c_long_long) :: kernel_launches
+        integer(c_int)       :: inner64_iters
       end type aphid_info
 
       interface
@@ -101,6 +103,7 @@
       opts%stream = c_null_ptr
       opts%graph_iters = 0
       opts%verbose = 0
+      opts%plane_kz = 0
       rc = aphid_gpu_create(ctx, opts)
       if (rc.ne.APHID_OK) then
         write(iout,*) '>> ERROR: no usable GPU for qmr_gpu, code ', rc

@@ -243,9 +243,10 @@ int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx);
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);
 
 /* Benchmarking hook, no counterpart in the reference: launch the fused
- * QMR iteration pass (complex64, or complex128 after a FUSED64 sweep) (p update, q^ = D^-1 K p^, the lagged d/x
- * update with zero weights, the inner products) `reps` times over all
- * systems of the last mixed-precision sweep, on the context's stream, without
+ * QMR iteration pass -- complex64, or complex128 after a FUSED64 sweep --
+ * (p update, q^ = D^-1 K p^, the lagged d/x update with zero weights, the
+ * inner products) `reps` times over all systems of the last batched sweep,
+ * on the context's stream, without
  * the scalar recurrence.  The solutions (aphid_gpu_sweep_fetch) are not
  * changed; the inner Krylov vectors are, as by an iteration.  Returns after
  * the launches (asynchronous). */

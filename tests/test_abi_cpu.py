@@ -103,3 +103,40 @@ def test_synthetic_models_shapes():
     assert np.all(m.sig_re[:, :, :8] == np.float32(1e-8))
     s = model.make_model("sweep128")
     assert len(s.systems()) == 96
+
+
+def _c_struct_fields(header, name):
+    import re
+    m = re.search(r"typedef struct \{([^{}]*)\} " + name + ";", header)
+    body = re.sub(r"/\*.*?\*/", "", m.group(1), flags=re.S)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        names = decl.split(None, 1)[1] if not decl.startswith("long long") else decl.split(None, 2)[2]
+        fields += [n.strip().lstrip("*") for n in names.split(",")]
+    return fields
+
+
+def _fortran_type_fields(src, name):
+    import re
+    m = re.search(r"type, bind\(C\) :: " + name + r"\n(.*?)end type " + name, src, re.S)
+    fields = []
+    for line in m.group(1).splitlines():
+        if "::" in line:
+            fields += [n.strip() for n in line.split("::", 1)[1].split(",")]
+    return fields
+
+
+def test_fortran_binding_types_match_the_c_structs():
+    """The ISO_C_BINDING module's bind(C) types carry the C structs' fields in
+    the same order (a missing trailing field makes the library read or write
+    past the Fortran variable)."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with open(os.path.join(root, "include", "aphid_gpu.h")) as f:
+        header = f.read()
+    with open(os.path.join(root, "aphid_git_b200", "fortran", "aphid_gpu_mod.f90")) as f:
+        src = f.read()
+    for name in ("aphid_opts", "aphid_info"):
+        assert _fortran_type_fields(src, name) == _c_struct_fields(header, name), name
