@@ -21,6 +21,10 @@
       integer(c_int), parameter :: APHID_OK = 0
       integer(c_int), parameter :: APHID_CONVERGED = 0
       integer(c_int), parameter :: APHID_MAXIT = 1
+      integer(c_int), parameter :: APHID_PREC_FP64 = 0
+      integer(c_int), parameter :: APHID_PREC_MIXED = 1
+      integer(c_int), parameter :: APHID_PREC_FUSED64 = 2
+      integer(c_int), parameter :: APHID_PREC_AUTO = 3
 
       type, bind(C) :: aphid_opts
         integer(c_int) :: device
@@ -37,6 +41,17 @@
         integer(c_long_long) :: kernel_launches
         integer(c_int)       :: inner64_iters
       end type aphid_info
+
+      ! options of aphid_gpu_sweep (the batched farm of aphid_parallel)
+      type, bind(C) :: aphid_sweep_opts
+        integer(c_int) :: precision
+        real(c_double) :: target
+        integer(c_int) :: max_it
+        real(c_double) :: inner_tol
+        integer(c_int) :: max_outer
+        integer(c_int) :: stall_window
+        integer(c_int) :: reserved(2)
+      end type aphid_sweep_opts
 
       interface
         integer(c_int) function aphid_gpu_create(ctx, opts)             &
@@ -80,6 +95,39 @@
           integer(c_int), value :: max_it, hist_cap
           real(c_double), intent(out) :: hist(*)
           type(aphid_info), intent(out) :: info
+        end function
+
+        ! cell model of a sweep: csig_flag 'R', 'C' or 'I' with the real(4)
+        ! cell arrays of read_mesh (c_null_ptr for an absent one)
+        integer(c_int) function aphid_gpu_set_model(ctx, csig_flag,     &
+                       sig_re, eps_rel)                                 &
+                       bind(C, name="aphid_gpu_set_model")
+          import :: c_int, c_ptr, c_char
+          type(c_ptr), value :: ctx
+          character(kind=c_char), value :: csig_flag
+          type(c_ptr), value :: sig_re, eps_rel
+        end function
+
+        ! every (frequency, source) system of aphid_mpi.freq / .source in
+        ! one call: omega(nsys), source_of_system(nsys) (0-based source
+        ! index), ndip(nsrc) dipoles per source, dip_dir(2*sum(ndip))
+        ! "+X".."-Z", dip_ijk(3*sum(ndip)) 1-based tail nodes; x_out
+        ! (nsys concatenated solutions) and x0 may be c_null_ptr
+        integer(c_int) function aphid_gpu_sweep(ctx, nsys, omega,        &
+                       source_of_system, nsrc, src_ndip, dip_dir,       &
+                       dip_ijk, x0, opts, x_out, info)                  &
+                       bind(C, name="aphid_gpu_sweep")
+          import :: c_int, c_ptr, c_double, c_char, aphid_sweep_opts,   &
+                    aphid_info
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: nsys, nsrc
+          real(c_double), intent(in) :: omega(*)
+          integer(c_int), intent(in) :: source_of_system(*), src_ndip(*)
+          character(kind=c_char), intent(in) :: dip_dir(*)
+          integer(c_int), intent(in) :: dip_ijk(*)
+          type(c_ptr), value :: x0, x_out
+          type(aphid_sweep_opts), intent(in) :: opts
+          type(aphid_info), intent(out) :: info(*)
         end function
       end interface
 

@@ -115,7 +115,7 @@ def _c_struct_fields(header, name):
         if not decl:
             continue
         names = decl.split(None, 1)[1] if not decl.startswith("long long") else decl.split(None, 2)[2]
-        fields += [n.strip().lstrip("*") for n in names.split(",")]
+        fields += [n.strip().lstrip("*").split("[")[0] for n in names.split(",")]
     return fields
 
 
@@ -125,7 +125,7 @@ def _fortran_type_fields(src, name):
     fields = []
     for line in m.group(1).splitlines():
         if "::" in line:
-            fields += [n.strip() for n in line.split("::", 1)[1].split(",")]
+            fields += [n.strip().split("(")[0] for n in line.split("::", 1)[1].split(",")]
     return fields
 
 
@@ -138,5 +138,5 @@ def test_fortran_binding_types_match_the_c_structs():
         header = f.read()
     with open(os.path.join(root, "aphid_git_b200", "fortran", "aphid_gpu_mod.f90")) as f:
         src = f.read()
-    for name in ("aphid_opts", "aphid_info"):
+    for name in ("aphid_opts", "aphid_info", "aphid_sweep_opts"):
         assert _fortran_type_fields(src, name) == _c_struct_fields(header, name), name
