@@ -1209,6 +1209,7 @@ SweepSys sweep_sys_init(double omega, const aphid_sweep_opts *opts, bool fused, 
   S.stall_window = opts->stall_window > 0 ? opts->stall_window
                    : (opts->stall_window < 0 || fused) ? INT_MAX : kStallWindow;
   S.escalate = escalate ? 1 : 0;
+  S.mon_level = fused ? 10.0 * opts->target : std::max(kMonitorLevel, 30.0 * opts->target);
   S.phase = PH_OUTER;
   S.status = -1;
   return S;

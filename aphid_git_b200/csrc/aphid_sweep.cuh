@@ -64,10 +64,12 @@ constexpr int kParts = 12;  // partial sums per slot and system
 // recurrence has reached its floor and only a restart from the FP64 residual
 // makes progress.
 constexpr double kStagnation = 16.0;
-// The monitor runs only once the quasi-residual predicts a true residual
-// (rnorm at the cycle start times tau / tau0) below this fraction of ||b||,
-// or below 30 x the target: above both, neither convergence nor the
-// complex64 floor (about 1e-6 ||b||) can have been reached.
+// For complex64 inner solves the monitor runs only once the quasi-residual
+// predicts a true residual (rnorm at the cycle start times tau / tau0) below
+// this fraction of ||b||, or below 30 x the target: above both, neither
+// convergence nor the complex64 floor (about 1e-6 ||b||) can have been
+// reached.  Complex128 inner solves track the true residual, so their monitor
+// waits for 10 x the target (SweepSys::mon_level).
 constexpr double kMonitorLevel = 1e-4;
 // rho_{n+1}^2 from the expansion ||q||^2 - 2 Re(conj(beta) v^H q) + |beta|^2
 // ||v||^2 is trusted down to this fraction of ||q||^2; below it the new
@@ -112,6 +114,7 @@ struct SweepSys {
   int stall_window;          // window length (INT_MAX: no stall test)
   int escalate;              // 1: end with kStEscalated when the bilinear form collapses
   int escalated;             // set by the pass; the outer step then ends the system
+  double mon_level;          // the monitor runs once the predicted true residual is below this x ||b||
 };
 
 // plane tile of the complex64 pass: 16 x 16 nodes marching along k; staged
@@ -795,7 +798,7 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
   const long long tile = blockIdx.x / D.nsys;
   SweepSys *S = D.sys + sys;
   if (S->phase != PH_INNER || S->inner_it < 2) return;
-  if (S->rnorm * (S->tau / S->tau0) > fmax(kMonitorLevel, 30.0 * S->target) * S->bnorm) return;
+  if (S->rnorm * (S->tau / S->tau0) > S->mon_level * S->bnorm) return;
   int i, j, k0, k1;
   sweep_tile(D, tile, i, j, k0, k1);
   Vals<1> a{{0.0}};
