@@ -146,6 +146,22 @@ def test_sweep_masking_keeps_systems_independent(solver):
     assert np.array_equal(solver.sweep_fetch(2), Xa[2])
 
 
+def test_sweep_writes_into_a_callers_array(solver):
+    """sweep(out=...) fills the caller's array (pinned host memory in the
+    benchmark) with the same solutions it returns, and rejects a wrong shape."""
+    xn, yn, zn, sig, _ = small_model(seed=7)
+    solver.set_nodes(xn, yn, zn)
+    solver.set_model("R", sig)
+    src = [[("+X", 6, 6, 4)]]
+    w = [2 * np.pi * f for f in (0.1, 10.0)]
+    X, _ = solver.sweep(w, src, [0, 0])
+    out = np.zeros_like(X)
+    Y, _ = solver.sweep(w, src, [0, 0], out=out)
+    assert Y is out and np.array_equal(out, X)
+    with pytest.raises(AphidError):
+        solver.sweep(w, src, [0, 0], out=np.zeros((1, X.shape[1]), np.complex128))
+
+
 def test_sweep_initial_guess(solver):
     xn, yn, zn, sig, _ = small_model(seed=4)
     solver.set_nodes(xn, yn, zn)
