@@ -1294,7 +1294,11 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
     return fail(ctx, APHID_ERR_NOMEM, "sweep: no memory to reorder escalated systems");
   }
   size_t fr = 0, tot = 0;
-  CK(cudaMemGetInfo(&fr, &tot));
+  const cudaError_t me = cudaMemGetInfo(&fr, &tot);
+  if (me != cudaSuccess) {
+    cudaFree(tmp);
+    return cuda_fail(ctx, me, "cudaMemGetInfo");
+  }
   const size_t per = 8 * 4 * (size_t)ctx->nl.N * sizeof(double2) + ((size_t)1 << 26);
   const size_t have = fr + (ctx->sw_w64 ? (size_t)ctx->sw_nsys64 * 8 * 4 * ctx->nl.N * sizeof(double2) : 0);
   const int cap = (int)std::max<size_t>(1, std::min<size_t>(esc.size(), (have - std::min(have, (size_t)1 << 30)) / per));
@@ -1338,11 +1342,16 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
       out[s] = I;
     }
   }
-  CK(cudaStreamSynchronize(ctx->stream));
+  const cudaError_t se = cudaStreamSynchronize(ctx->stream);
   cudaFree(tmp);
-  // the complex128 buffers are sized for this phase only
+  // the complex128 buffers were sized for this phase only: release them, so
+  // that the next mixed sweep has the memory it had
   if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
   ctx->sw_gexec = nullptr;
+  cudaFree(ctx->sw_w64);
+  ctx->sw_w64 = nullptr;
+  ctx->sw_nsys64 = 0;
+  if (!rc && se != cudaSuccess) rc = cuda_fail(ctx, se, "sweep (escalated systems)");
   return rc;
 }
 
