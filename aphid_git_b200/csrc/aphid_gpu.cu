@@ -1106,7 +1106,7 @@ int sweep_graph(aphid_ctx *ctx, const SweepDev &D, bool fused64) {
 // (mesh, batch, model kind) in the process and, when the environment
 // variable APHID_TUNE_CACHE names a file, across processes (one line
 // "nx ny nz nsys eps kz" per shape).
-typedef std::array<int, 5> TuneKey;  // nx, ny, nz, nsys, eps-bar present
+typedef std::array<int, 5> TuneKey;  // nx, ny, nz, nsys, eps-bar present + 2 x complex128 pass
 
 std::mutex &tune_mutex() {
   static std::mutex m;
@@ -1138,8 +1138,8 @@ void tune_file_store(const TuneKey &k, int kz) {
   std::fclose(f);
 }
 
-int tune_kz(aphid_ctx *ctx, int nsys) {
-  const TuneKey key = {ctx->nx, ctx->ny, ctx->nz, nsys, ctx->d_epsr32 ? 1 : 0};
+int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
+  const TuneKey key = {ctx->nx, ctx->ny, ctx->nz, nsys, (ctx->d_epsr32 ? 1 : 0) + (fused ? 2 : 0)};
   int kz = 0;
   {
     std::lock_guard<std::mutex> lock(tune_mutex());
@@ -1164,9 +1164,15 @@ int tune_kz(aphid_ctx *ctx, int nsys) {
       if ((rc = plane_tiles(ctx, c))) return rc;
       SweepDev D = sweep_dev(ctx, nsys);
       D.tmix = 0.f;
-      for (int r = 0; r < 2; r++) launch_pass(ctx, D, true);
+      auto pass = [&]() {
+        if (fused)
+          launch_pass64(ctx, D, true);
+        else
+          launch_pass(ctx, D, true);
+      };
+      for (int r = 0; r < 2; r++) pass();
       CK(cudaEventRecord(ctx->ev0, ctx->stream));
-      for (int r = 0; r < 5; r++) launch_pass(ctx, D, true);
+      for (int r = 0; r < 5; r++) pass();
       CK(cudaEventRecord(ctx->ev1, ctx->stream));
       CK(cudaEventSynchronize(ctx->ev1));
       CK(cudaGetLastError());
@@ -1176,7 +1182,7 @@ int tune_kz(aphid_ctx *ctx, int nsys) {
         kz = c;
         best_ms = ms;
       }
-      if (ctx->verbose) std::fprintf(stderr, "aphid_gpu: tune kz=%d %.3f ms/pass\n", c, ms / 5);
+      if (ctx->verbose) std::fprintf(stderr, "aphid_gpu: tune kz=%d %.3f ms/pass%s\n", c, ms / 5, fused ? " (c128)" : "");
     }
     int kerr = 0;
     CK(cudaMemcpy(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1305,6 +1311,7 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
   for (size_t c0 = 0; c0 < esc.size() && !rc; c0 += cap) {
     const int k = (int)std::min<size_t>(cap, esc.size() - c0);
     if ((rc = sweep_alloc64(ctx, k))) break;
+    if (ctx->plane_kz <= 0 && (rc = tune_kz(ctx, k, true))) break;
     // slot of each system, and the swaps that bring this chunk to the front
     std::vector<int> slot_of(ctx->sw_nsys), sys_at(ctx->sw_nsys);
     for (int q = 0; q < ctx->sw_nsys; q++) slot_of[q] = sys_at[q] = q;
@@ -1486,11 +1493,11 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
   if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
   if (fused && (rc = sweep_alloc64(ctx, nsys))) return rc;
   if ((rc = ensure_work(ctx))) return rc;
-  if (mixed) {
+  if (mixed || fused) {
     if (ctx->plane_kz > 0) {
       if (ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) && (rc = plane_tiles(ctx, ctx->plane_kz)))
         return rc;
-    } else if ((rc = tune_kz(ctx, nsys))) {
+    } else if ((rc = tune_kz(ctx, nsys, fused))) {
       return rc;
     }
   }
