@@ -248,7 +248,9 @@ int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);
  * inner products) `reps` times over all systems of the last batched sweep,
  * on the context's stream, without
  * the scalar recurrence.  The solutions (aphid_gpu_sweep_fetch) are not
- * changed; the inner Krylov vectors are, as by an iteration.  Returns after
+ * changed; the inner Krylov vectors are, as by an iteration.  An AUTO sweep
+ * that escalated systems releases its inner buffers, so after one this returns
+ * APHID_ERR_STATE until the next MIXED, AUTO or FUSED64 sweep.  Returns after
  * the launches (asynchronous). */
 int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps);
 
