@@ -33,6 +33,12 @@ class SweepOpts(C.Structure):
                 ("reserved", C.c_int * 2)]
 
 
+class Source(C.Structure):
+    """aphid_source: oper_mode 2 / 3 (MT sheet sources) or 5 (dipole list)"""
+    _fields_ = [("oper_mode", C.c_int), ("ndip", C.c_int), ("dip_dir", C.c_char_p),
+                ("dip_ijk", C.c_void_p)]
+
+
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("stream", C.c_void_p), ("graph_iters", C.c_int),
                 ("verbose", C.c_int), ("plane_kz", C.c_int)]
@@ -87,6 +93,8 @@ def load():
     L.aphid_gpu_set_model.argtypes = [P, C.c_char, P, P]
     L.aphid_gpu_sweep.argtypes = [P, C.c_int, P, P, C.c_int, P, C.c_char_p, P, P,
                                   C.POINTER(SweepOpts), P, P]
+    L.aphid_gpu_sweep_sources.argtypes = [P, C.c_int, P, P, C.c_int, P, P, C.POINTER(SweepOpts), P, P]
+    L.aphid_gpu_sweep_receivers.argtypes = [P, C.c_int, P, P, P]
     L.aphid_gpu_sweep_fetch.argtypes = [P, C.c_int, P]
     L.aphid_gpu_sweep_time_apply.argtypes = [P, C.c_int]
     L.aphid_gpu_sweep_apply.argtypes = [P, _Z, _Z]
@@ -112,6 +120,28 @@ def _c128(a, n=None):
     if n is not None and a.size != n:
         raise ValueError("expected %d complex values, got %d" % (n, a.size))
     return a
+
+
+def _sources(sources):
+    """aphid_source array for a list of sources (dipole lists or the MT
+    oper_mode 2 / 3); returns (array, buffers to keep alive)"""
+    arr = (Source * len(sources))()
+    keep = []
+    for q, src in enumerate(sources):
+        if isinstance(src, (int, np.integer)) and not isinstance(src, bool):
+            if int(src) not in (2, 3):
+                raise AphidError("an integer source must be oper_mode 2 or 3 (MT), got %r" % (src,))
+            arr[q].oper_mode = int(src)
+            continue
+        dips = list(src)
+        dirs = "".join(str(d[0])[:2].ljust(2) for d in dips).encode() or b"  "
+        ijk = np.array([[int(d[1]), int(d[2]), int(d[3])] for d in dips] or [[0, 0, 0]], dtype=np.int32)
+        keep += [dirs, ijk]
+        arr[q].oper_mode = 5
+        arr[q].ndip = len(dips)
+        arr[q].dip_dir = dirs
+        arr[q].dip_ijk = ijk.ctypes.data
+    return arr, keep
 
 
 NOALLOC_MAX_NODES = 1024
@@ -140,6 +170,7 @@ class Solver:
         if rc != APHID_OK:
             raise AphidError("aphid_gpu_create failed: %s" % ERRORS.get(rc, rc))
         self.dims = None
+        self._last_nsys = 0
 
     def close(self):
         if self._h:
@@ -285,8 +316,10 @@ class Solver:
               out=None):
         """Solve all (omega, source) systems in one batched launch.
 
-        sources: list of oper_mode-5 dipole lists [(dir, i, j, k), ...];
-        source_of_system[s] picks the source of system s (default: s).
+        sources: one entry per source, each an oper_mode-5 dipole list
+        [(dir, i, j, k), ...] or the integer 2 or 3 (the x- or y-polarised
+        MT sheet source of gen_rhs); source_of_system[s] picks the source of
+        system s (default: s).
         precision: "auto" (complex64 inner solves; systems whose Lanczos
         bilinear form collapses below complex64 resolution finish in
         complex128), "mixed", "fused64" (complex128 inner solves, same
@@ -300,10 +333,7 @@ class Solver:
         nsys = om.size
         sos = np.ascontiguousarray(np.arange(nsys) if source_of_system is None
                                    else source_of_system, dtype=np.int32)
-        ndip = np.array([len(q) for q in sources], dtype=np.int32)
-        dirs = "".join(str(d[0])[:2].ljust(2) for q in sources for d in q).encode()
-        ijk = np.array([[int(d[1]), int(d[2]), int(d[3])] for q in sources for d in q] or
-                       [[0, 0, 0]], dtype=np.int32)
+        srcs, keep = _sources(sources)
         x0a = None if x0 is None else np.ascontiguousarray(x0, dtype=np.complex128).reshape(nsys, self.n)
         if out is not None:
             if (out.dtype != np.complex128 or out.shape != (nsys, self.n) or not out.flags["C_CONTIGUOUS"]):
@@ -312,15 +342,33 @@ class Solver:
         else:
             X = np.empty((nsys, self.n), np.complex128) if fetch else None
         infos = (Info * nsys)()
+        self._last_nsys = 0
         if precision not in PRECISIONS:
             raise AphidError("precision must be one of %s" % ", ".join(PRECISIONS))
         o = SweepOpts(PRECISIONS[precision], float(target), int(max_it),
                       float(inner_tol), int(max_outer), int(stall_window))
-        self._check(self.lib.aphid_gpu_sweep(
-            self._h, nsys, om.ctypes.data, sos.ctypes.data, len(sources), ndip.ctypes.data,
-            dirs or b"  ", ijk.ctypes.data, x0a.ctypes.data if x0a is not None else None,
+        self._check(self.lib.aphid_gpu_sweep_sources(
+            self._h, nsys, om.ctypes.data, sos.ctypes.data, len(sources), srcs,
+            x0a.ctypes.data if x0a is not None else None,
             C.byref(o), X.ctypes.data if X is not None else None, infos), "sweep")
+        del keep
+        self._last_nsys = nsys
         return X, [i.as_dict() for i in infos]
+
+    def sweep_receivers(self, rec_ijk, e=True, h=True):
+        """E and H at receiver nodes for every system of the last sweep
+        (aphid_gpu_sweep_receivers): rec_ijk is (nrec, 3) 1-based interior
+        nodes; returns (E, H), each (nsys, nrec, 3) complex128 or None."""
+        rec = np.ascontiguousarray(np.atleast_2d(rec_ijk), dtype=np.int32)
+        if rec.ndim != 2 or rec.shape[1] != 3:
+            raise ValueError("rec_ijk must be (nrec, 3)")
+        nsys = self._last_nsys
+        E = np.empty((nsys, len(rec), 3), np.complex128) if e else None
+        H = np.empty((nsys, len(rec), 3), np.complex128) if h else None
+        self._check(self.lib.aphid_gpu_sweep_receivers(
+            self._h, len(rec), rec.ctypes.data, E.ctypes.data if e else None,
+            H.ctypes.data if h else None), "sweep_receivers")
+        return E, H
 
     def sweep_time_apply(self, reps):
         """Launch the fused complex64 QMR pass `reps` times on the resident

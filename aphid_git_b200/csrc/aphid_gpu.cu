@@ -5,6 +5,8 @@
 // the QMR iteration.  All arithmetic of the solve runs on the GPU; there is no
 // CPU fallback (a missing or unsupported device is an error).
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <array>
@@ -92,6 +94,7 @@ struct aphid_ctx {
   long long sw_slots = 0;
   int sw_bps = 0;
   int sw_last = 0;           // systems in the last sweep
+  std::vector<double> sw_omega;  // their angular frequencies
   bool sw_last_fused = false; // its inner storage was complex128 (FUSED64)
   cudaGraphExec_t sw_gexec = nullptr;
   int sw_gkey = 0;
@@ -895,8 +898,12 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     cudaFree(ctx->sw_cnt);
     ctx->sw_f64 = nullptr;
     ctx->sw_f32 = nullptr;
+    ctx->sw_sys = nullptr;
+    ctx->sw_part = nullptr;
+    ctx->sw_cnt = nullptr;
     ctx->sw_f32_ok = false;
     ctx->sw_nsys = 0;
+    ctx->sw_last = 0;
     const size_t vec = (size_t)nsys * ctx->n;
     if (cudaMalloc(&ctx->sw_f64, 2 * vec * sizeof(double2)) != cudaSuccess) {
       cudaGetLastError();
@@ -970,17 +977,39 @@ int sweep_alloc64(aphid_ctx *ctx, int k) {
   return vector_maps64(ctx);
 }
 
-// oper_mode 5 sources (src/aphid.f90:638-741) as sparse (index, value) lists
-// per source, duplicates accumulated in file order.
-void source_entries(const aphid_ctx *ctx, int nsrc, const int *src_ndip, const char *dir, const int *ijk,
+// Sources (gen_rhs, src/aphid.f90:534-743) as sparse (index, value) lists
+// per source.  oper_mode 2 / 3: the x- / y-polarised MT sheet current on node
+// layer k = 2 (src/aphid.f90:590-619), mu0 dx(i) (dy(j-1) + dy(j)) / 2 on the
+// x-edges (mu0 dy(j) (dx(i-1) + dx(i)) / 2 on the y-edges), multiplied in the
+// reference's order.  oper_mode 5: dipole lists (:638-741), duplicates
+// accumulated in file order.
+void source_entries(const aphid_ctx *ctx, int nsrc, const aphid_source *srcs,
                     std::vector<std::map<long long, double>> &out) {
   const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
   const int lim[3] = {nx, ny, nz};
   const long long off[3] = {ctx->g.ox, ctx->g.oy, ctx->g.oz};
+  const std::vector<double> &dx = ctx->host_d[0], &dy = ctx->host_d[1];
   out.assign(nsrc, {});
-  long long pos = 0;
   for (int q = 0; q < nsrc; q++) {
-    for (int m = 0; m < src_ndip[q]; m++, pos++) {
+    const aphid_source &S = srcs[q];
+    if (S.oper_mode == 2) {
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx - 1; i++)
+          out[q][ctx->g.ox + i + (long long)(nx - 1) * (j + (long long)ny * 1)] =
+              kMu0 * dx[i + 1] * (0.5 * (dy[j] + dy[j + 1]));
+      continue;
+    }
+    if (S.oper_mode == 3) {
+      for (int j = 0; j < ny - 1; j++)
+        for (int i = 0; i < nx; i++)
+          out[q][ctx->g.oy + i + (long long)nx * (j + (long long)(ny - 1) * 1)] =
+              kMu0 * dy[j + 1] * (0.5 * (dx[i] + dx[i + 1]));
+      continue;
+    }
+    const char *dir = S.dip_dir;
+    const int *ijk = S.dip_ijk;
+    for (int m = 0; m < S.ndip; m++) {
+      const long long pos = m;
       const char s0 = dir[2 * pos], s1 = dir[2 * pos + 1];
       if (!((s0 == '+' || s0 == '-') && (s1 == 'X' || s1 == 'Y' || s1 == 'Z'))) continue;
       const int a = s1 - 'X';
@@ -1103,10 +1132,14 @@ int sweep_graph(aphid_ctx *ctx, const SweepDev &D, bool fused64) {
 // The z-slab depth of the complex64 pass is chosen by timing the pass itself
 // (timing launches over the resident buffers, which leave the solver state
 // alone) for each candidate depth on this mesh and batch, and cached per
-// (mesh, batch, model kind) in the process and, when the environment
+// (mesh, batch, model kind, device) in the process and, when the environment
 // variable APHID_TUNE_CACHE names a file, across processes (one line
-// "nx ny nz nsys eps kz" per shape).
-typedef std::array<int, 5> TuneKey;  // nx, ny, nz, nsys, eps-bar present + 2 x complex128 pass
+// "nx ny nz nsys kind sms dev kz" per shape, written with one append so that
+// processes sharing the file cannot interleave a record; lines that do not
+// parse are ignored).  The device is identified by its multiprocessor count
+// and a hash of its name, so ranks on different GPU models keep their own
+// choices.
+typedef std::array<int, 7> TuneKey;  // nx, ny, nz, nsys, eps-bar present + 2 x complex128 pass, SMs, name hash
 
 std::mutex &tune_mutex() {
   static std::mutex m;
@@ -1122,9 +1155,18 @@ int tune_file_lookup(const TuneKey &k) {
   if (!path || !*path) return 0;
   FILE *f = std::fopen(path, "r");
   if (!f) return 0;
-  int v[6], found = 0;
-  while (std::fscanf(f, "%d %d %d %d %d %d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) == 6)
-    if (v[0] == k[0] && v[1] == k[1] && v[2] == k[2] && v[3] == k[3] && v[4] == k[4] && v[5] >= kMinKz) found = v[5];
+  char line[256];
+  int found = 0;
+  while (std::fgets(line, sizeof line, f)) {
+    int v[8];
+    char tail;
+    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %c", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7],
+                    &tail) != 8)
+      continue;  // torn, foreign or old-format record
+    bool same = v[7] >= kMinKz;
+    for (int q = 0; q < 7; q++) same = same && v[q] == k[q];
+    if (same) found = v[7];
+  }
   std::fclose(f);
   return found;
 }
@@ -1132,14 +1174,35 @@ int tune_file_lookup(const TuneKey &k) {
 void tune_file_store(const TuneKey &k, int kz) {
   const char *path = std::getenv("APHID_TUNE_CACHE");
   if (!path || !*path) return;
-  FILE *f = std::fopen(path, "a");
-  if (!f) return;
-  std::fprintf(f, "%d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4], kz);
-  std::fclose(f);
+  char line[160];
+  const int len = std::snprintf(line, sizeof line, "%d %d %d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4], k[5],
+                                k[6], kz);
+  if (len <= 0 || len >= (int)sizeof line) return;
+  const int fd = ::open(path, O_WRONLY | O_APPEND | O_CREAT, 0644);
+  if (fd < 0) return;
+  const ssize_t w = ::write(fd, line, (size_t)len);  // one append: the record lands whole
+  (void)w;
+  ::close(fd);
+}
+
+// device identity of the tune key: multiprocessor count and a hash of the name
+void device_identity(const aphid_ctx *ctx, int &sms, int &name_hash) {
+  cudaDeviceProp prop;
+  sms = ctx->num_sms;
+  name_hash = 0;
+  if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  unsigned h = 2166136261u;  // FNV-1a
+  for (const char *c = prop.name; *c; c++) h = (h ^ (unsigned char)*c) * 16777619u;
+  name_hash = (int)(h & 0x7fffffff);
 }
 
 int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
-  const TuneKey key = {ctx->nx, ctx->ny, ctx->nz, nsys, (ctx->d_epsr32 ? 1 : 0) + (fused ? 2 : 0)};
+  int sms, name_hash;
+  device_identity(ctx, sms, name_hash);
+  const TuneKey key = {ctx->nx, ctx->ny, ctx->nz, nsys, (ctx->d_epsr32 ? 1 : 0) + (fused ? 2 : 0), sms, name_hash};
   int kz = 0;
   {
     std::lock_guard<std::mutex> lock(tune_mutex());
@@ -1469,15 +1532,37 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
                     const aphid_sweep_opts *opts, aphid_z *x_out, aphid_info *info) {
   int rc = check_ready(ctx);
   if (rc) return rc;
-  if (!ctx->has_model) return fail(ctx, APHID_ERR_STATE, "aphid_gpu_set_model has not been called");
-  if (nsys < 1 || nsrc < 1 || !omega || !source_of_system || !src_ndip || !opts || !info)
-    return fail(ctx, APHID_ERR_BADARG, "sweep: bad counts or null arrays");
-  long long ndip = 0;
+  if (nsrc < 1 || !src_ndip) return fail(ctx, APHID_ERR_BADARG, "sweep: bad counts or null arrays");
+  std::vector<aphid_source> srcs(nsrc);
+  long long pos = 0;
   for (int q = 0; q < nsrc; q++) {
     if (src_ndip[q] < 0) return fail(ctx, APHID_ERR_BADARG, "negative dipole count");
-    ndip += src_ndip[q];
+    if (src_ndip[q] > 0 && (!dip_dir || !dip_ijk)) return fail(ctx, APHID_ERR_BADARG, "null dipole arrays");
+    srcs[q].oper_mode = 5;
+    srcs[q].ndip = src_ndip[q];
+    srcs[q].dip_dir = dip_dir ? dip_dir + 2 * pos : nullptr;
+    srcs[q].dip_ijk = dip_ijk ? dip_ijk + 3 * pos : nullptr;
+    pos += src_ndip[q];
   }
-  if (ndip > 0 && (!dip_dir || !dip_ijk)) return fail(ctx, APHID_ERR_BADARG, "null dipole arrays");
+  return aphid_gpu_sweep_sources(ctx, nsys, omega, source_of_system, nsrc, srcs.data(), x0, opts, x_out, info);
+}
+
+int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega, const int *source_of_system, int nsrc,
+                            const aphid_source *srcs, const aphid_z *x0, const aphid_sweep_opts *opts,
+                            aphid_z *x_out, aphid_info *info) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->has_model) return fail(ctx, APHID_ERR_STATE, "aphid_gpu_set_model has not been called");
+  if (nsys < 1 || nsrc < 1 || !omega || !source_of_system || !srcs || !opts || !info)
+    return fail(ctx, APHID_ERR_BADARG, "sweep: bad counts or null arrays");
+  for (int q = 0; q < nsrc; q++) {
+    const aphid_source &S = srcs[q];
+    if (S.oper_mode != 2 && S.oper_mode != 3 && S.oper_mode != 5)
+      return fail(ctx, APHID_ERR_BADARG, "sweep: a source's oper_mode must be 2, 3 or 5");
+    if (S.oper_mode == 5 && S.ndip < 0) return fail(ctx, APHID_ERR_BADARG, "negative dipole count");
+    if (S.oper_mode == 5 && S.ndip > 0 && (!S.dip_dir || !S.dip_ijk))
+      return fail(ctx, APHID_ERR_BADARG, "null dipole arrays");
+  }
   for (int s = 0; s < nsys; s++) {
     if (source_of_system[s] < 0 || source_of_system[s] >= nsrc)
       return fail(ctx, APHID_ERR_BADARG, "source index out of range");
@@ -1490,6 +1575,9 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
   if (!(opts->target >= 0.0) || opts->max_it < 0) return fail(ctx, APHID_ERR_BADARG, "bad target or max_it");
   if ((mixed || fused) && 4 * ctx->nl.N >= (1LL << 31))
     return fail(ctx, APHID_ERR_BADARG, "batched sweep: more than 2^31 node-layout values per system");
+  // from here on the buffers are rebuilt for this call: until it succeeds,
+  // the post-sweep hooks (time_apply, apply, fetch) must refuse the old state
+  ctx->sw_last = 0;
   if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
   if (fused && (rc = sweep_alloc64(ctx, nsys))) return rc;
   if ((rc = ensure_work(ctx))) return rc;
@@ -1504,7 +1592,7 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
 
   // sources -> sparse right-hand sides
   std::vector<std::map<long long, double>> src;
-  source_entries(ctx, nsrc, src_ndip, dip_dir, dip_ijk, src);
+  source_entries(ctx, nsrc, srcs, src);
   std::vector<long long> eidx;
   std::vector<double> eval;
   for (int s = 0; s < nsys; s++)
@@ -1582,6 +1670,7 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
   }
   ctx->sw_last = nsys;
   ctx->sw_last_fused = fused;
+  ctx->sw_omega.assign(omega, omega + nsys);
   if (x_out) {
     CK(cudaMemcpyAsync(x_out, x64, vec * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1625,6 +1714,54 @@ int aphid_gpu_sweep_apply(aphid_ctx *ctx, const aphid_z *x, aphid_z *y) {
   }
   if (!ctx->sw_f32_ok) return fail(ctx, APHID_ERR_STATE, "no complex64 sweep state on the device");
   return sweep_apply_t<float2>(ctx, x, y);
+}
+
+int aphid_gpu_sweep_receivers(aphid_ctx *ctx, int nrec, const int *rec_ijk, aphid_z *E, aphid_z *H) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (ctx->sw_last < 1 || (int)ctx->sw_omega.size() != ctx->sw_last)
+    return fail(ctx, APHID_ERR_STATE, "no batched sweep on the device");
+  if (nrec < 1 || !rec_ijk || (!E && !H)) return fail(ctx, APHID_ERR_BADARG, "receivers: bad count or null arrays");
+  std::vector<int> rec(3 * (size_t)nrec);
+  const int lim[3] = {ctx->nx, ctx->ny, ctx->nz};
+  for (int r = 0; r < nrec; r++)
+    for (int c = 0; c < 3; c++) {
+      const int v = rec_ijk[3 * r + c] - 1;  // 0-based
+      if (v < 1 || v > lim[c] - 2) return fail(ctx, APHID_ERR_BADARG, "receivers: nodes must be interior (2..n-1)");
+      rec[3 * r + c] = v;
+    }
+  const int nsys = ctx->sw_last;
+  const size_t nout = (size_t)nsys * nrec * 3;
+  int *d_rec = nullptr;
+  double *d_om = nullptr;
+  double2 *d_out = nullptr;
+  cudaError_t e = cudaMalloc(&d_rec, rec.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_om, nsys * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, 2 * nout * sizeof(double2));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_rec, rec.data(), rec.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_om, ctx->sw_omega.data(), nsys * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    const long long cnt = (long long)nsys * nrec;
+    k_receivers<<<(unsigned)((cnt + 127) / 128), 128, 0, ctx->stream>>>(ctx->g, ctx->sw_f64, ctx->n, d_om, nsys, nrec,
+                                                                         d_rec, E ? d_out : nullptr,
+                                                                         H ? d_out + nout : nullptr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && E) e = cudaMemcpyAsync(E, d_out, nout * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && H)
+    e = cudaMemcpyAsync(H, d_out + nout, nout * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_rec);
+  cudaFree(d_om);
+  cudaFree(d_out);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, e == cudaErrorMemoryAllocation ? APHID_ERR_NOMEM : APHID_ERR_CUDA,
+                std::string("receivers: ") + cudaGetErrorString(e));
+  }
+  return APHID_OK;
 }
 
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x) {

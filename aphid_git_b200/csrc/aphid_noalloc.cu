@@ -12,13 +12,15 @@
 // That array is loaded with the library and held by every GPU that uses it
 // until the process exits.  All calls share it and it keeps the contents of
 // the last call: calls that overlap on the GPU (different streams, or
-// different host threads on the same device) race on it.  The first call on
-// each device looks up the array's device address (cudaGetSymbolAddress);
-// make that first call before any stream capture.
+// different host threads on the same device) race on it.  Every call looks up
+// the array's device address in the current context (cudaGetSymbolAddress, a
+// host-side lookup), so a context made after cudaDeviceReset, or another
+// context current on the device, gets its own copy's address.  The first call
+// on a device also loads the library's kernels there: make it before any
+// stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "../../include/aphid_gpu.h"
 #include "aphid_qmr64.cuh"
@@ -36,10 +38,6 @@ constexpr size_t kScratchDoubles = kCntOff + 2;
 
 // tables (3 axes) | partials (2 doubles per slot) | ticket counter
 static __device__ __align__(256) double g_scratch[kScratchDoubles];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double *g_addr[kMaxDevices] = {};  // device address of g_scratch, per device
 
 // Coefficient tables of one axis into the scratch, the same formulas as the
 // context path's host-side tables (gen_inprod_*_coefs, src/aphid.f90:750-1185):
@@ -80,22 +78,19 @@ extern "C" int aphid_gpu_inprod_eps_noalloc(int nx, int ny, int nz, const double
   if (!d_dx || !d_dy || !d_dz || !d_dxc || !d_dyc || !d_dzc || !d_k2 || !d_in || !d_out || !d_eps)
     return APHID_ERR_BADARG;
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return APHID_ERR_NODEVICE;
-
-  double *scratch;
-  {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {  // once per device, with that device current
-      void *p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-      if (e != cudaSuccess || !p) {
-        cudaGetLastError();
-        return APHID_ERR_CUDA;
-      }
-      g_addr[dev] = (double *)p;
-    }
-    scratch = g_addr[dev];
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
+    cudaGetLastError();
+    return APHID_ERR_NODEVICE;
   }
+  // the array's address in the context current now (host code cannot use
+  // the symbol itself: its host-side name is not a device address)
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return APHID_ERR_CUDA;
+  }
+  double *scratch = (double *)p;
   cudaStream_t st = (cudaStream_t)stream;
 
   GridDev g{};

@@ -299,4 +299,68 @@ static __global__ void k_fields(GridDev g, double omega, const double2 *__restri
     ez[ixz(g, i, j, k) - g.oz] = E(a[ixz(g, i, j, k)], a[pc + (long long)nx * ny], a[pc], dzk);
 }
 
+// ------------------------------------------------------------- receivers
+// E and H at mesh nodes with the node interpolation of dump_fields' EM_grid
+// output (src/aphid.f90:2012-2165): E along each axis is the mean of the two
+// edges through the node, B of each component the mean of the four faces
+// around it, H = B / mu0.  (EM_grid's By_grid line repeats the face
+// By(i, j, k-1) in place of By(i-1, j, k); the mean here is over the four
+// distinct faces.)  The face and edge values are those of k_fields, formed
+// with the same operations.
+__device__ __forceinline__ double2 face_bx(const GridDev &g, const double2 *a, int i, int j, int k) {
+  const double dyj = g.ax[1].d[j + 1], dzk = g.ax[2].d[k + 1];
+  return cadd(csub(csub(rdiv(a[ixz(g, i, j + 1, k)], dyj), rdiv(a[ixy(g, i, j, k + 1)], dzk)),
+                   rdiv(a[ixz(g, i, j, k)], dyj)),
+              rdiv(a[ixy(g, i, j, k)], dzk));
+}
+__device__ __forceinline__ double2 face_by(const GridDev &g, const double2 *a, int i, int j, int k) {
+  const double dxi = g.ax[0].d[i + 1], dzk = g.ax[2].d[k + 1];
+  return cadd(csub(csub(rdiv(a[ixx(g, i, j, k + 1)], dzk), rdiv(a[ixz(g, i + 1, j, k)], dxi)),
+                   rdiv(a[ixx(g, i, j, k)], dzk)),
+              rdiv(a[ixz(g, i, j, k)], dxi));
+}
+__device__ __forceinline__ double2 face_bz(const GridDev &g, const double2 *a, int i, int j, int k) {
+  const double dxi = g.ax[0].d[i + 1], dyj = g.ax[1].d[j + 1];
+  return cadd(csub(csub(rdiv(a[ixy(g, i + 1, j, k)], dxi), rdiv(a[ixx(g, i, j + 1, k)], dyj)),
+                   rdiv(a[ixy(g, i, j, k)], dxi)),
+              rdiv(a[ixx(g, i, j, k)], dyj));
+}
+// E on the edge of component c (0, 1, 2) that starts at node (i, j, k)
+__device__ __forceinline__ double2 edge_e(const GridDev &g, const double2 *a, double omega, int c, int i, int j,
+                                          int k) {
+  const long long pc = ixp(g, i, j, k);
+  const long long t = c == 0 ? ixx(g, i, j, k) : (c == 1 ? ixy(g, i, j, k) : ixz(g, i, j, k));
+  const long long step = c == 0 ? 1 : (c == 1 ? (long long)g.nx : (long long)g.nx * g.ny);
+  const double h = g.ax[c].d[(c == 0 ? i : (c == 1 ? j : k)) + 1];
+  const double2 w = csub(a[t], rdiv(csub(a[pc + step], a[pc]), h));
+  return make_double2(omega * w.y, -(omega * w.x));  // -(i omega w)
+}
+
+// one thread per (system, receiver): rec holds 0-based interior nodes
+// (i, j, k), 1 <= i <= nx-2 etc.; E, H are [nsys][nrec][3]
+static __global__ void k_receivers(GridDev g, const double2 *__restrict__ x, long long n, const double *__restrict__ omega,
+                                   int nsys, int nrec, const int *__restrict__ rec, double2 *__restrict__ E,
+                                   double2 *__restrict__ H) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nsys * nrec) return;
+  const int s = (int)(t / nrec), r = (int)(t % nrec);
+  const int i = rec[3 * r], j = rec[3 * r + 1], k = rec[3 * r + 2];
+  const double2 *a = x + (long long)s * n;
+  const double w = omega[s];
+  if (E) {
+    E[3 * t] = rmul(0.5, cadd(edge_e(g, a, w, 0, i - 1, j, k), edge_e(g, a, w, 0, i, j, k)));
+    E[3 * t + 1] = rmul(0.5, cadd(edge_e(g, a, w, 1, i, j - 1, k), edge_e(g, a, w, 1, i, j, k)));
+    E[3 * t + 2] = rmul(0.5, cadd(edge_e(g, a, w, 2, i, j, k - 1), edge_e(g, a, w, 2, i, j, k)));
+  }
+  if (H) {
+    const double q = 0.25 / kMu0;
+    H[3 * t] = rmul(q, cadd(cadd(face_bx(g, a, i, j - 1, k - 1), face_bx(g, a, i, j, k - 1)),
+                            cadd(face_bx(g, a, i, j - 1, k), face_bx(g, a, i, j, k))));
+    H[3 * t + 1] = rmul(q, cadd(cadd(face_by(g, a, i - 1, j, k - 1), face_by(g, a, i, j, k - 1)),
+                                cadd(face_by(g, a, i - 1, j, k), face_by(g, a, i, j, k))));
+    H[3 * t + 2] = rmul(q, cadd(cadd(face_bz(g, a, i - 1, j - 1, k), face_bz(g, a, i, j - 1, k)),
+                                cadd(face_bz(g, a, i - 1, j, k), face_bz(g, a, i, j, k))));
+  }
+}
+
 }  // namespace aphid

@@ -158,6 +158,11 @@
         stop
       end if
       rc = aphid_gpu_set_mesh(ctx, nx, ny, nz, dx, dy, dz, dxc, dyc, dzc)
+      if (rc.ne.APHID_OK) then
+        write(iout,*) '>> ERROR: aphid_gpu_set_mesh failed, code ', rc
+        rc = aphid_gpu_destroy(ctx)
+        stop
+      end if
       allocate(hist(max(1, qmr_max_it)))
       rc = aphid_gpu_qmr(ctx, k2_xgrid, k2_ygrid, k2_zgrid, k2_pgrid,   &
                          diag_x, diag_y, diag_z, diag_p,                &

@@ -279,6 +279,42 @@ def read_mpi_source(path):
     return arrays
 
 
+def write_mpi_freq(path, freqs):
+    """aphid_mpi.freq in the layout read_mpi_freq (and the farm) reads"""
+    bar = "=" * 72
+    with open(path, "w") as f:
+        f.write("%s\nAPHID: source frequency array [Hz]\n%s\n" % (bar, bar))
+        f.write("%-13d! number of frequencies\n" % len(freqs))
+        for v in freqs:
+            f.write("%-13.6e\n" % v)
+
+
+def write_mpi_input(path, source_type, qmr_target, qmr_max_it, csig_flag="R"):
+    """aphid_mpi.input: MT or CS, QMR target, iteration cap, model flag"""
+    bar = "=" * 72
+    with open(path, "w") as f:
+        f.write("%s\nAPHID Input File: Operational parameters for PARALLEL MPI computation\n%s\n" % (bar, bar))
+        f.write("%-10s!! mode of operation (either 'MT', or 'CS' for dipole array)\n" % source_type)
+        f.write("%-10.3e!! QMR target residual\n" % qmr_target)
+        f.write("%-10d!! max QMR iterates\n" % qmr_max_it)
+        f.write("%-10s!! conductivity model: [R]eal, [C]omplex, [D]ispersive, [I]nsulator\n" % csig_flag)
+
+
+def write_mpi_source(path, arrays):
+    """aphid_mpi.source: the dipole arrays of a CS sweep, each a list of
+    (dir, i, j, k), in the block layout the farm reads"""
+    bar = "=" * 72
+    with open(path, "w") as f:
+        f.write("%s\nAPHID: list of controlled-source electric dipole array sources\n%s\n" % (bar, bar))
+        f.write("%-15d!  number of dipole arrays\n\n" % len(arrays))
+        for arr in arrays:
+            f.write("%s\ndipole array definition\n%s\n" % (bar, bar))
+            f.write("%-15d! number of elementary dipoles in array\n" % len(arr))
+            for d, i, j, k in arr:
+                f.write("%s %d %d %d\n" % (d, i, j, k))
+            f.write("\n")
+
+
 def sweep_systems(freqs, source_type, dipole_arrays=None):
     """The (frequency, source) list the MPI farm distributes
     (src/aphid_parallel.f90:75-103): MT gives modes 2 and 3 per frequency,
@@ -366,6 +402,45 @@ def _earth(cshape, nair, rng, nblocks=20, corr=8.0):
         e[lo[0]:lo[0] + sz[0], lo[1]:lo[1] + sz[1], lo[2]:lo[2] + sz[2]] = 10.0 ** rng.uniform(-4, 1)
     sig[:, :, nair:] = e
     return sig
+
+
+def _e12_4(v):
+    """values as Fortran's e12.4 edit descriptor prints them (5 significant
+    digits), which is how gen_mesh.f90 writes aphid.mesh"""
+    return np.array([float("%12.4e" % x) for x in np.asarray(v, np.float32)])
+
+
+def serial_mt_model(nh=50):
+    """The reference's serial MT example (serial/gen_mesh.f90), the 1-D
+    layered-earth check of the paper: nh x nh x 121 nodes.  Horizontally
+    uniform 200 km / 49 cells (nh = 50 reproduces the file; any nh >= 3
+    gives the same laterally uniform solution under an MT sheet source).
+    Vertically 51 air cells of 100 km / 51 above z = 0, then 19 cells of
+    1 km, 20 of 50 m and 30 of 1 km down to 50 km, node coordinates
+    accumulated in real(4) and rounded as e12.4 writes them.  Cell
+    conductivity by cell-centre depth: air 1e-8 S/m, 0.001 S/m down to
+    19 km, 0.1 S/m to 20 km, 0.01 S/m below (gen_mesh.f90's loop, in which
+    the shallower conditions override the deeper ones).  Returns (xn, yn,
+    zn, sig_re (nh-1, nh-1, 120) real(4), index of the surface node)."""
+    nair, near = 51, 69
+    z = np.zeros(nair + near + 1, np.float32)
+    z[0] = -100e3
+    dza = np.float32(100e3) / np.float32(nair)
+    for i in range(1, nair + 1):
+        z[i] = z[i - 1] + dza
+    for i in range(nair + 1, nair + near + 1):
+        f = i + 1  # Fortran index
+        small = nair + 2 + 19 <= f < nair + 41
+        z[i] = z[i - 1] + (np.float32(50.0) if small else np.float32(1e3))
+    h = np.float32(200e3) / np.float32(49)
+    x = np.float32(-100e3) + h * np.arange(nh, dtype=np.float32)
+    zc = 0.5 * (z[:-1] + z[1:])
+    sc = np.full(zc.shape, 0.01, np.float32)
+    sc[zc < 20e3] = 0.10
+    sc[zc < 19e3] = 0.001
+    sc[zc < 0.0] = 1e-8
+    sig = np.broadcast_to(sc[None, None, :], (nh - 1, nh - 1, len(zc))).astype(np.float32)
+    return _e12_4(x), _e12_4(x), _e12_4(z), np.asfortranarray(sig), nair
 
 
 def make_model(config, seed=None):

@@ -1,19 +1,50 @@
-"""Benchmark: time-to-residual-1e-8 of APhiD's frequency-domain solve on B200.
+"""Benchmark: time-to-residual-1e-8 of a whole frequency sweep of APhiD's
+frequency-domain solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload hetero96] [--precision fp64]
+                    [--workload seafloor256] [--precision auto]
 
-One step = one full solve of the workload to relative residual 1e-8 from a
-zero start.  `value` = sweeps per second over all ranks, measured on device
-with CUDA events, inputs resident in HBM (aphid_gpu_qmr_run); `e2e` = the same
-through the public host-buffer call (aphid_gpu_qmr: host->device copies of
-k^2, the Jacobi diagonal and b, device->host copy of the solution, inside the
-timed region).  The working set (10 complex128 vectors of 3.6 M unknowns,
-580 MB) is larger than L2, so no explicit flush is needed.
+Workload (default): seafloor256, the full-scale configuration -- 256 x 256 x
+192 cells (50.8 M unknowns per system), 10 air layers over 15 layers of
+3.3 S/m seawater over a heterogeneous earth, one +X dipole on the sea floor,
+24 frequencies log-spaced 1e-3..1e5 Hz.  One step is one sweep: all 24
+systems solved from a zero start to a true FP64 relative residual of 1e-8,
+batched in one persistent solve (aphid_gpu_sweep), AUTO precision (complex64
+inner QMR in FP64 defect correction; systems whose Lanczos form collapses in
+complex64 finish in complex128).
 
-Multi-GPU: one process per GPU, each solving its own sweep (the reference's
-MPI farm is an embarrassingly parallel split over frequencies x sources), no
-collective in the solve; value = sweeps of all ranks / max-over-ranks time.
+  value   sweeps/s with the model resident on the device (Solver.sweep, the
+          solutions left on the device), K timed sweeps between CUDA events;
+          the working set (about 120 GB) is far larger than L2, no flush.
+  e2e     the same call with host buffers: the real(4) conductivity uploaded
+          from pinned host memory and all solutions copied into a pinned host
+          array inside the timed region (--e2e-steps sweeps, default 2).
+  plain_fp64_sweep / fused64_sweep
+          the same 24 systems through the reference's own complex128
+          recurrence one system at a time (aphid_gpu_qmr path) and through the
+          batched complex128 pass, timed once each; the speed-ups are their
+          times over ours.
+  field_err
+          E and H at sea-floor receivers of the AUTO solutions against
+          complex128 solves to 1e-12 (low, middle and high frequency).
+  roofline
+          the fused complex64 pass (k_sw_pass), timed with CUDA events on the
+          sweep's stream over timing launches on the resident batch; plus the
+          pass's effective bandwidth over a whole sweep.
+  cpu_baseline / --impl reference
+          the oracle's 4-thread component split (the reference's qmr_mthread
+          parallelism, OMP_NUM_THREADS=4) on 4 pinned host cores, timed over a
+          bounded sample of QMR iterations of the workload and extrapolated
+          with the per-system complex128 iteration counts (measured in this
+          run by the plain sweep; the reference arm, which runs no GPU code,
+          uses the counts recorded by `bench.py --record-fp64-iters` in
+          profiles/fp64_iters.json).
+
+Multi-GPU: one process per GPU; the systems of the sweep are dealt to the
+ranks by predicted cost (aphid_git_b200.farm, the reference's MPI farm split
+over frequencies x sources), no collective in the solve, receiver values
+gathered to rank 0; value = sweeps / max-over-ranks time ("strong": the total
+work is one sweep at every N).
 """
 import argparse
 import json
@@ -21,7 +52,6 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -32,11 +62,8 @@ sys.path.insert(0, ROOT)
 METRIC = "time-to-residual-1e-8 per frequency sweep (reported as sweeps/s) and QMR iters/s"
 TARGET = 1e-8
 MAX_IT = 20000
-# Iterations to relative residual 1e-8 of the complex128 Jacobi-QMR (the
-# reference's own recurrence and stop test) on each workload, measured on the
-# B200 complex128 path, which reproduces the reference's iteration count.  The
-# CPU arms time a bounded number of iterations and extrapolate with it.
-FP64_ITERS = {"halfspace32": 360, "hetero96": 1088}
+ITERS_FILE = os.path.join(ROOT, "profiles", "fp64_iters.json")
+CPU_THREADS = 4
 
 
 def peaks():
@@ -95,97 +122,143 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def setup_problem(workload):
+# ------------------------------------------------------------ workload
+def systems_of(m):
+    """(omega, source index) of every system, frequencies fastest, as the
+    reference's MPI farm orders them (src/aphid_parallel.f90:97-101)."""
+    om, sos = [], []
+    for q in range(len(m.sources)):
+        for f in m.freqs:
+            om.append(2 * np.pi * float(f))
+            sos.append(q)
+    return om, sos
+
+
+def receivers_of(m):
+    """sea-floor (or surface) receivers: the nodes on the source's node layer
+    along x through the source, every 4th node of the interior"""
+    nx, ny, nz = m.dims
+    _, _, jc, ks = m.sources[0][0]
+    return np.array([[i, jc, ks] for i in range(2, nx, 4)], np.int32)
+
+
+# ------------------------------------------------------------ CPU arms
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def pin_cores(n=CPU_THREADS):
+    """pin this process to its first n allowed cores (the OpenMP threads the
+    oracle starts afterwards inherit the mask); returns (cores, old mask)"""
+    old = sorted(os.sched_getaffinity(0))
+    cores = old[:n]
+    os.sched_setaffinity(0, cores)
+    return cores, old
+
+
+def cpu_sample(m, iters, threads=CPU_THREADS):
+    """seconds per QMR iteration of the oracle's 4-thread component split
+    (the reference's qmr_mthread parallelism, src/aphid_qmr.f90:744-928) on
+    the first system of the workload, on pinned cores: two runs of a and
+    a + iters iterations, s/iter = (t(a + iters) - t(a)) / iters, so that the
+    fixed start-up of a solve (thread spin-up, first touch of the work
+    vectors, the initial residual) is not charged to the iterations.  (A
+    plain short run over-states the steady rate: 6 iterations on hetero96
+    gave 0.149 s/iter against 0.061 s/iter over a full 1082-iteration
+    solve.)  Returns (s/iter, iterations timed, cores)."""
     from aphid_git_b200 import model
-    m = model.make_model(workload)
-    w = 2 * np.pi * float(m.freqs[0])
-    sig = model.sigma_hat("R", w, m.sig_re.ravel(order="F"))
-    b, _ = model.gen_rhs(m.xn, m.yn, m.zn, 5, m.sources[0])
-    return m, w, sig, b
-
-
-def cpu_port_sample(workload, iters, threads=4):
-    """The oracle's 4-thread component split (the reference's qmr_mthread
-    parallelism, src/aphid_qmr.f90:744-928) for `iters` iterations.
-    Returns seconds per iteration."""
     from oracle import oracle as O
-    m, w, sig, b = setup_problem(workload)
-    g = O.Grid(m.xn, m.yn, m.zn)
-    k2 = O.gen_k2(g, sig, w)
-    diag = O.gen_diag(g, k2)
-    r = O.qmr(g, k2, diag, b, 1e-30, iters, nthreads=threads)
-    return r["seconds"] / max(1, len(r["hist"])), len(r["hist"])
+    cores, old = pin_cores(threads)
+    try:
+        w = 2 * np.pi * float(m.freqs[0])
+        sig = model.sigma_hat("R", w, m.sig_re.ravel(order="F"))
+        b, _ = model.gen_rhs(m.xn, m.yn, m.zn, 5, m.sources[0])
+        g = O.Grid(m.xn, m.yn, m.zn)
+        k2 = O.gen_k2(g, sig, w)
+        diag = O.gen_diag(g, k2)
+        a = 3
+        ra = O.qmr(g, k2, diag, b, 1e-30, a, nthreads=threads)
+        rb = O.qmr(g, k2, diag, b, 1e-30, a + iters, nthreads=threads)
+        done = len(rb["hist"]) - len(ra["hist"])
+        return max(rb["seconds"] - ra["seconds"], 1e-9) / max(1, done), done, cores
+    finally:
+        os.sched_setaffinity(0, old)
+
+
+def recorded_iters(workload):
+    try:
+        with open(ITERS_FILE) as f:
+            d = json.load(f)[workload]
+        return [int(v) for v in d["iters"]], d.get("source", "")
+    except Exception:
+        return None, None
+
+
+def cpu_baseline_obj(spi, done, cores, iters, iters_src, nsys_per_sweep):
+    total = int(sum(iters))
+    return {"value": 1.0 / (spi * total), "unit": "sweeps/s", "cores": len(cores), "kind": "port",
+            "cpu": cpu_model(), "pinned_cores": cores, "s_per_iter": spi,
+            "sample": "%d QMR iterations of the first system (difference of a 3- and a longer run), "
+                      "oracle 4-thread component split on %d pinned cores; time-to-tolerance "
+                      "extrapolated = %.3f s/iter x %d complex128 "
+                      "iterations summed over the %d systems (%s)"
+                      % (done, len(cores), spi, total, nsys_per_sweep, iters_src)}
 
 
 def run_reference(args):
-    """--impl reference: the CPU port of the reference's path (no Fortran
-    compiler exists here, so oracle/_ref cannot be built)."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    """--impl reference: the CPU restatement of the reference's path (the
+    reference is Fortran + MPI; no Fortran compiler exists here, so no
+    oracle/_ref), timed on this host's cores.  Rank 0 only."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    iters = FP64_ITERS.get(args.workload)
     from aphid_git_b200 import model
     m = model.make_model(args.workload)
-    sample_it = args.cpu_sample_iters
-    times = []
+    om, _ = systems_of(m)
+    iters, src = recorded_iters(args.workload)
+    if iters is None or len(iters) != len(om):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "no recorded complex128 iteration counts for %s in profiles/fp64_iters.json "
+                          "(run bench.py --record-fp64-iters on a GPU)" % args.workload}))
+        return 0
+    times, done, cores = [], 0, []
     for step in range(args.warmup + args.steps):
-        spi, done = cpu_port_sample(args.workload, sample_it)
+        spi, done, cores = cpu_sample(m, args.cpu_sample_iters)
         if step >= args.warmup:
             times.append(spi)
     spi = float(np.mean(times))
-    value = 1.0 / (spi * iters) if iters else None
+    cb = cpu_baseline_obj(spi, done, cores, iters, "recorded on B200 in " + os.path.basename(ITERS_FILE)
+                          + ": " + src, len(om))
+    value = cb["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": spi * iters * 1e3 if iters else None, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": {"workload": args.workload, "precision": "complex128 (the reference's algorithm, CPU)",
-                   "unknowns": int(m.n), "systems": len(systems_of(m)[0]), "target": TARGET,
+                   "unknowns": int(m.n), "systems": len(om), "target": TARGET,
                    "parallelism": "one process, 4 threads (qmr_mthread component split)"},
-        "s_per_iter": spi, "iters_to_tol": iters,
-        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": 4, "kind": "port",
-                         "sample": "%d QMR iterations per step, 4-thread component split; "
-                                   "time-to-tolerance = s/iter x %s iterations" % (sample_it, iters)},
-        "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
+        "s_per_iter": spi, "iters_to_tol": iters, "extrapolated": True,
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
+# ------------------------------------------------------------ GPU arm
 def pass_bytes(nsys, n):
     """Algorithmic bytes of one fused complex64 QMR pass over a batch: per
     unknown and system read q^, v^, p^, d^, x^ and write q^, v^, p^, d^, x^
     (10 x 8 B; the Jacobi diagonal is formed on chip), plus the shared FP32
     sigma-bar once (4 B)."""
     return nsys * n * 80 + n * 4
-
-
-def time_apply(s, k2, n, dev, stream, reps=50):
-    """Seconds per launch of the QMR-step operator apply (q = K p and
-    epsilon = p^T q in one pass) on the library's stream, CUDA events."""
-    import torch
-    kt = torch.from_numpy(k2.view(np.float64)).to(dev)
-    pt = torch.randn(2 * n, dtype=torch.float64, device=dev)
-    qt = torch.empty(2 * n, dtype=torch.float64, device=dev)
-    et = torch.empty(2, dtype=torch.float64, device=dev)
-    torch.cuda.synchronize(dev)
-    for _ in range(5):
-        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        s.inprod_dev(kt.data_ptr(), pt.data_ptr(), qt.data_ptr(), et.data_ptr())
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    return e0.elapsed_time(e1) * 1e-3 / reps
-
-
-def only_apply(s, k2, n, dev, stream):
-    t = time_apply(s, k2, n, dev, stream, reps=10)
-    print(json.dumps({"apply_us": t * 1e6, "unknowns": n, "alg_GBps": 48 * n / t / 1e9}))
-    return 0
 
 
 def timed(stream, dev, fn, steps, barrier, world):
@@ -209,15 +282,20 @@ def timed(stream, dev, fn, steps, barrier, world):
     return ms, out
 
 
-def systems_of(m):
-    """(omega, source index) of every system, frequencies fastest, as the
-    reference's MPI farm orders them (src/aphid_parallel.f90:97-101)."""
-    om, sos = [], []
-    for q in range(len(m.sources)):
-        for f in m.freqs:
-            om.append(2 * np.pi * float(f))
-            sos.append(q)
-    return om, sos
+def field_error(s, m, om, sos, rec, Ea, Ha, idx):
+    """relative error of E and H at the receivers of systems idx (from a
+    finished sweep: Ea, Ha) against complex128 solves of the reference's
+    recurrence to 1e-12"""
+    s.sweep([om[q] for q in idx], m.sources, [sos[q] for q in idx], precision="fp64",
+            target=1e-12, max_it=4 * MAX_IT, fetch=False)
+    Er, Hr = s.sweep_receivers(rec)
+    err = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    e = [err(Ea[q], Er[r]) for r, q in enumerate(idx)]
+    h = [err(Ha[q], Hr[r]) for r, q in enumerate(idx)]
+    return {"E": max(e), "H": max(h), "per_system": {"freq_hz": [om[q] / (2 * np.pi) for q in idx],
+                                                      "E": e, "H": h},
+            "reference": "complex128 Jacobi-QMR (reference recurrence) to 1e-12",
+            "receivers": int(len(rec))}
 
 
 def main():
@@ -226,20 +304,21 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hetero96")
-    ap.add_argument("--precision", default="auto", choices=["mixed", "auto", "fused64", "fp64"])
-    ap.add_argument("--plain-sweep", action="store_true",
-                    help="also time the plain complex128 path over every system of the workload "
-                         "(one solve each, the reference's algorithm) and report the ratio")
+    ap.add_argument("--workload", default="seafloor256")
+    ap.add_argument("--precision", default="auto", choices=["mixed", "auto", "fused64"])
     ap.add_argument("--inner-tol", type=float, default=0.0)
-    ap.add_argument("--plain-steps", type=int, default=2,
-                    help="timed complex128 solves for the speed-up comparison (0: skip)")
-    ap.add_argument("--cpu-sample-iters", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain complex128 sweep")
+    ap.add_argument("--no-fused64", action="store_true", help="skip the batched complex128 sweep")
+    ap.add_argument("--no-field-err", action="store_true")
+    ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--record-fp64-iters", action="store_true",
+                    help="write the plain sweep's per-system iteration counts to profiles/fp64_iters.json")
     ap.add_argument("--one-sweep", action="store_true",
-                    help="run one mixed sweep of the workload and exit (profiling target)")
+                    help="run one sweep of the workload and exit (profiling target)")
     ap.add_argument("--only-apply", action="store_true",
-                    help="set up the workload and time only the operator apply (profiling)")
+                    help="set up the workload and time only the fused pass (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -248,7 +327,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from aphid_git_b200 import Solver
+    from aphid_git_b200 import Solver, farm, model
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -256,11 +335,10 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    # a real stream (not the NULL stream) shared by the library and the
-    # CUDA events, so the events bracket the library's kernels
+    # a real stream shared by the library and the CUDA events
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
 
@@ -268,182 +346,160 @@ def main():
         if world > 1:
             dist.barrier()
 
-    m, w, sig, b = setup_problem(args.workload)
+    m = model.make_model(args.workload)
     s = Solver(device=local, stream=stream.cuda_stream)
     s.set_nodes(m.xn, m.yn, m.zn)
     n = s.n
     om, sos = systems_of(m)
     nsys = len(om)
+    rec = receivers_of(m)
+    parts = farm.assign(farm.predicted_cost(np.array(om) / (2 * np.pi)), world)
+    mine = parts[rank]
+    my_om, my_sos = [om[q] for q in mine], [sos[q] for q in mine]
     peak, peak_kind = peaks()
-    clocks = ClockSampler(local)
+    s.set_model("R", m.sig_re)
+
+    def sweep(prec=args.precision, out=None):
+        if not mine:
+            return []
+        return s.sweep(my_om, m.sources, my_sos, precision=prec, target=TARGET, max_it=MAX_IT,
+                       inner_tol=args.inner_tol, fetch=False if out is None else True, out=out)[1]
 
     if args.one_sweep:
-        # one mixed sweep of the workload, nothing timed (profiling target)
-        s.set_model("R", m.sig_re)
-        prec = "mixed" if args.precision == "fp64" else args.precision
-        _, inf = s.sweep(om, m.sources, sos, precision=prec, target=TARGET, max_it=MAX_IT, fetch=False)
-        print(json.dumps({"workload": args.workload, "precision": prec, "systems": nsys, "plane_kz": s.sweep_plane_kz(),
-                          "inner_iters": [i["inner_iters"] for i in inf][:8],
-                          "outer_iters": [i["outer_iters"] for i in inf][:8],
-                          "inner64_iters": [i["inner64_iters"] for i in inf][:8],
+        inf = sweep()
+        print(json.dumps({"workload": args.workload, "precision": args.precision, "systems": len(mine),
+                          "plane_kz": s.sweep_plane_kz(),
+                          "inner_iters": [i["inner_iters"] for i in inf],
+                          "inner64_iters": [i["inner64_iters"] for i in inf],
                           "seconds": inf[0]["seconds"], "launches": inf[0]["kernel_launches"]}))
         return 0
-
-    if args.only_apply and args.precision == "mixed":
-        # resident complex64 state from a short sweep, then the operator pass
-        s.set_model("R", m.sig_re)
-        s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=8, fetch=False)
+    if args.only_apply:
+        sweep("mixed" if args.precision == "auto" else args.precision)
         ms_a, _ = timed(stream, dev, lambda: s.sweep_time_apply(10), 1, lambda: None, 1)
         t = ms_a * 1e-3 / 10
-        print(json.dumps({"apply_us": t * 1e6, "unknowns": n, "systems": nsys,
-                          "alg_GBps": pass_bytes(nsys, n) / t / 1e9}))
+        print(json.dumps({"apply_us": t * 1e6, "unknowns": n, "systems": len(mine),
+                          "alg_GBps": pass_bytes(len(mine), n) / t / 1e9}))
         return 0
 
-    plain = None
-    if args.precision == "fp64" or args.only_apply or args.plain_steps > 0:
-        # the plain complex128 path: the reference's algorithm, one system at
-        # a time, inputs resident (k^2, Jacobi diagonal and b on the device)
-        k2 = s.gen_k2(sig, w)
-        diag = s.gen_diag(k2)
-        if args.only_apply:
-            return only_apply(s, k2, n, dev, stream)
-        s.qmr_load(k2, diag, b)
-        s.qmr_run(TARGET, MAX_IT)
-        steps = args.steps if args.precision == "fp64" else args.plain_steps
-        if args.precision == "fp64":
-            for _ in range(args.warmup - 1):
-                s.qmr_run(TARGET, MAX_IT)
-            clocks.start()
-            time.sleep(0.3)
-        ms_p, inf_p = timed(stream, dev, lambda: s.qmr_run(TARGET, MAX_IT)[0], steps, barrier, world)
-        plain = {"time_to_tol_s": ms_p / steps * 1e-3, "iters_to_tol": inf_p[-1]["iters"],
-                 "true_rel_resid": inf_p[-1]["true_rel_resid"],
-                 "launches": int(sum(i["kernel_launches"] for i in inf_p)), "ms": ms_p,
-                 "steps": steps, "note": "complex128 Jacobi-QMR, reference recurrence, "
-                 "first system of the workload"}
+    # ---- the timed region: K sweeps, inputs resident
+    for _ in range(args.warmup):
+        sweep()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ms, infs = timed(stream, dev, sweep, args.steps, barrier, world)
+    clk = clocks.stop()
+    last = infs[-1]
+    launches = int(sum(i[0]["kernel_launches"] for i in infs if i))
+    value = args.steps / (ms * 1e-3)
+    Ea, Ha = s.sweep_receivers(rec) if mine else (None, None)
 
-    if args.precision == "fp64":
-        clk = clocks.stop()
-        ms, launches = plain["ms"], plain["launches"]
-        iters = plain["iters_to_tol"]
-        value = world * args.steps / (ms * 1e-3)
-        ms_e, _ = timed(stream, dev, lambda: s.qmr(k2, diag, b, TARGET, MAX_IT, hist=False)[1],
-                        args.steps, barrier, world)
-        e2e = {"value": world * args.steps / (ms_e * 1e-3), "unit": "sweeps/s",
-               "h2d_bytes_per_step": 3 * 16 * n, "d2h_bytes_per_step": 16 * n}
-        t_apply = time_apply(s, k2, n, dev, stream)
-        alg = 3 * 16 * n
-        kernel = "k_apply64 (complex128 QMR step: q = K p, epsilon)"
-        extra = {"time_to_tol_s": ms / args.steps * 1e-3, "iters_to_tol": iters,
-                 "qmr_iters_per_s": world * args.steps * iters / (ms * 1e-3),
-                 "true_rel_resid": plain["true_rel_resid"]}
-        dtype = "c128"
-        traffic_key = "apply64_qmr_" + args.workload
-    else:
-        # the product path: batched mixed-precision sweep of all systems
-        s.set_model("R", m.sig_re)
+    # ---- e2e: host buffers, copies inside the timed region
+    sig_host = torch.empty(m.sig_re.shape[::-1], dtype=torch.float32, pin_memory=True).numpy().T
+    sig_host[...] = m.sig_re
+    x_host = torch.empty((max(1, len(mine)), n), dtype=torch.complex128, pin_memory=True).numpy()
 
-        def run_sweep():
-            return s.sweep(om, m.sources, sos, precision=args.precision, target=TARGET, max_it=MAX_IT,
-                           inner_tol=args.inner_tol, fetch=False)[1]
+    def run_e2e():
+        s.set_model("R", sig_host)
+        return sweep(out=x_host[:len(mine)])
 
-        for _ in range(args.warmup):
-            run_sweep()
-        clocks.start()
-        time.sleep(0.3)
-        ms, infs = timed(stream, dev, run_sweep, args.steps, barrier, world)
-        clk = clocks.stop()
-        last = infs[-1]
-        launches = int(sum(i[0]["kernel_launches"] for i in infs))
-        value = world * args.steps / (ms * 1e-3)
+    e2e_steps = max(1, args.e2e_steps)
+    ms_e, _ = timed(stream, dev, run_e2e, e2e_steps, barrier, world)
+    e2e = {"value": e2e_steps / (ms_e * 1e-3), "unit": "sweeps/s", "steps": e2e_steps,
+           "h2d_bytes_per_step": 4 * m.ncell, "d2h_bytes_per_step": 16 * n * len(mine),
+           "note": "real(4) conductivity host->device and every solution device->host (pinned) "
+                   "inside the timed region"}
+    del x_host
 
-        # host buffers in pinned memory, as a caller streaming many models would keep them
-        sig_host = torch.empty(m.sig_re.shape[::-1], dtype=torch.float32, pin_memory=True).numpy().T
-        sig_host[...] = m.sig_re
-        x_host = torch.empty((nsys, n), dtype=torch.complex128, pin_memory=True).numpy()
+    it_in = [i["inner_iters"] for i in last]
+    extra = {"time_to_tol_s": ms / args.steps * 1e-3, "systems": nsys, "systems_this_rank": len(mine),
+             "inner_iters": it_in, "inner_iters_total": int(sum(it_in)),
+             "inner64_iters_total": int(sum(i["inner64_iters"] for i in last)),
+             "outer_iters_max": max(i["outer_iters"] for i in last) if last else 0,
+             "qmr_iters_per_s": world * sum(it_in) / (ms / args.steps * 1e-3),
+             "cell_updates_per_s": world * sum(it_in) * m.ncell / (ms / args.steps * 1e-3),
+             "true_rel_resid_max": max(i["true_rel_resid"] for i in last) if last else None,
+             "status": sorted({i["status_name"] for i in last}), "plane_kz": s.sweep_plane_kz()}
 
-        def run_e2e():
-            s.set_model("R", sig_host)
-            return s.sweep(om, m.sources, sos, precision=args.precision, target=TARGET, max_it=MAX_IT,
-                           inner_tol=args.inner_tol, out=x_host)[1]
-
-        ms_e, _ = timed(stream, dev, run_e2e, args.steps, barrier, world)
-        e2e = {"value": world * args.steps / (ms_e * 1e-3), "unit": "sweeps/s",
-               "h2d_bytes_per_step": 4 * m.ncell, "d2h_bytes_per_step": 16 * n * nsys}
-        # dominant kernel: the fused complex64 QMR iteration (one launch per
-        # inner iteration); algorithmic bytes per launch in pass_bytes().
-        reps = 20
-        if args.precision == "auto":
-            # escalation releases the complex64 state: rebuild it for the timing launches
-            s.sweep(om, m.sources, sos, precision="mixed", target=TARGET, max_it=8, fetch=False)
-        s.sweep_time_apply(3)
-        ms_a, _ = timed(stream, dev, lambda: s.sweep_time_apply(reps), 1, lambda: None, 1)
-        t_apply = ms_a * 1e-3 / reps
-        f64 = args.precision == "fused64"
-        alg = pass_bytes(nsys, n) * (2 if f64 else 1)
-        kernel = ("k_sw_pass64 (fused complex128 QMR iteration" if f64 else
-                  "k_sw_pass (fused complex64 QMR iteration") + (
-                  ": p^ update, q^ = D^-1 K p^, lagged d^/x^ update, 12 inner products)")
-        it_in = [i["inner_iters"] for i in last]
-        extra = {"time_to_tol_s": ms / args.steps * 1e-3, "systems": nsys,
-                 "inner_iters_max": max(it_in), "inner_iters_total": int(sum(it_in)),
-                 "outer_iters_max": max(i["outer_iters"] for i in last),
-                 "qmr_iters_per_s": world * args.steps * sum(it_in) / (ms * 1e-3),
-                 "inner64_iters_total": int(sum(i["inner64_iters"] for i in last)),
-                 "true_rel_resid_max": max(i["true_rel_resid"] for i in last),
-                 "status": sorted({i["status_name"] for i in last})}
-        if args.plain_sweep:
-            # the plain complex128 path over every system, once
-            ms_p, inf_p = timed(stream, dev, lambda: s.sweep(om, m.sources, sos, precision="fp64", target=TARGET,
-                                                              max_it=MAX_IT, fetch=False)[1], 1, barrier, world)
-            pi = inf_p[-1]
-            extra["plain_fp64_sweep"] = {
-                "time_s": ms_p * 1e-3, "iters": [i["iters"] for i in pi],
-                "status": sorted({i["status_name"] for i in pi}),
-                "note": "complex128 Jacobi-QMR, the reference's recurrence and stop test, one system "
-                        "at a time on the same GPU"}
-            extra["speedup_vs_plain_fp64_sweep"] = ms_p * 1e-3 / (ms / args.steps * 1e-3)
-            extra["inner_iters"] = it_in
-        if plain is not None:
-            extra["plain_fp64"] = plain
-            extra["speedup_vs_plain_fp64"] = plain["time_to_tol_s"] * nsys / (ms / args.steps * 1e-3)
-        dtype = {"mixed": "c64 inner / f64 outer", "fused64": "c128 inner / f64 outer",
-                 "auto": "c64 inner (c128 after escalation) / f64 outer"}[args.precision]
-        traffic_key = ("sw_pass64_" if f64 else "sw_pass_") + args.workload
-
+    # ---- the dominant kernel: the fused complex64 pass
+    reps = 10
+    if mine:  # the complex64 state of the whole batch (AUTO releases it after escalation)
+        s.sweep(my_om, m.sources, my_sos, precision="mixed", target=TARGET, max_it=8, fetch=False)
+        s.sweep_time_apply(2)
+    ms_a, _ = timed(stream, dev, lambda: s.sweep_time_apply(reps) if mine else None, 1, lambda: None, 1)
+    t_apply = max(ms_a, 1e-9) * 1e-3 / reps
+    alg = pass_bytes(len(mine), n)
     achieved = alg / t_apply / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get(traffic_key)
+            traffic = json.load(f).get("sw_pass_" + args.workload)
+    roofline = {"bound": "hbm", "kernel": "k_sw_pass (fused complex64 QMR iteration: p^ update, "
+                "q^ = D^-1 K p^, lagged d^/x^ update, 12 inner products)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
+                "traffic": traffic, "alg_bytes_per_launch": alg, "launch_us": t_apply * 1e6,
+                "systems_per_launch": len(mine),
+                "units": "80 B per unknown and system + 4 B sigma-bar per unknown"}
+
+    # ---- comparisons on the same GPU (rank 0's share at N > 1)
+    if not args.no_plain:  # every rank takes the same collective steps
+        ms_p, inf_p = timed(stream, dev, lambda: sweep("fp64"), 1, barrier, world)
+        pi = inf_p[-1] or [{"iters": 0, "status_name": "none"}]
+        extra["plain_fp64_sweep"] = {
+            "time_s": ms_p * 1e-3, "iters": [i["iters"] for i in pi],
+            "status": sorted({i["status_name"] for i in pi}),
+            "note": "complex128 Jacobi-QMR, the reference's recurrence and stop test, one system at a "
+                    "time on the same GPU (k_apply64 + streaming kernels, graph-captured)"}
+        extra["speedup_vs_plain_fp64_sweep"] = ms_p / (ms / args.steps)
+        if args.record_fp64_iters and world == 1:
+            d = {}
+            if os.path.exists(ITERS_FILE):
+                with open(ITERS_FILE) as f:
+                    d = json.load(f)
+            d[args.workload] = {"iters": [i["iters"] for i in pi], "freq_hz": [w / (2 * np.pi) for w in om],
+                                "source": "bench.py --workload %s --record-fp64-iters, plain complex128 sweep "
+                                          "on %s" % (args.workload, torch.cuda.get_device_name(dev))}
+            with open(ITERS_FILE, "w") as f:
+                json.dump(d, f, indent=1)
+    if not args.no_fused64:
+        ms_f, inf_f = timed(stream, dev, lambda: sweep("fused64"), 1, barrier, world)
+        fi = inf_f[-1] or [{"inner_iters": 0, "status_name": "none"}]
+        extra["fused64_sweep"] = {"time_s": ms_f * 1e-3, "iters": [i["inner_iters"] for i in fi],
+                                  "status": sorted({i["status_name"] for i in fi}),
+                                  "note": "batched complex128 pass (k_sw_pass64) for every system"}
+        extra["speedup_vs_fused64_sweep"] = ms_f / (ms / args.steps)
+    if not args.no_field_err and mine:
+        idx = sorted({0, len(mine) // 2, len(mine) - 1})
+        extra["field_err"] = field_error(s, m, my_om, my_sos, rec, Ea, Ha, idx)
+    # effective bandwidth of the pass over a whole sweep (all kernels' time)
+    extra["sweep_effective_GBps"] = (sum(it_in) * 80.0 * n) / (ms / args.steps * 1e-3) / 1e9
+
     line = {
         "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": {"mixed": "c64 inner / f64 outer", "fused64": "c128 inner / f64 outer",
+                  "auto": "c64 inner (c128 after escalation) / f64 outer"}[args.precision],
         "data": "synthetic (seeded generator, no public dataset)",
         "config": {"workload": args.workload, "precision": args.precision, "unknowns": n,
-                   "systems": nsys, "target": TARGET,
+                   "systems": nsys, "target": TARGET, "max_it": MAX_IT,
                    "l2": "working set > L2 (126 MB), no flush",
-                   "parallelism": "independent sweep per GPU"},
-        "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
-                     "traffic": traffic, "alg_bytes_per_launch": alg,
-                     "launch_us": t_apply * 1e6},
+                   "parallelism": "systems dealt to ranks (farm), one batched sweep per rank"},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roofline,
     }
     line.update(extra)
-    iters_ref = FP64_ITERS.get(args.workload)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and iters_ref:
-        spi, done = cpu_port_sample(args.workload, args.cpu_sample_iters)
-        line["cpu_baseline"] = {
-            "value": 1.0 / (spi * iters_ref * nsys), "unit": "sweeps/s", "cores": 4,
-            "kind": "port",
-            "sample": "%d QMR iterations of the workload, oracle 4-thread component split; "
-                      "time-to-tolerance = %.3f s/iter x %d iterations (complex128 count, same "
-                      "recurrence) x %d systems" % (done, spi, iters_ref, nsys),
-            "s_per_iter": spi}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        iters = extra.get("plain_fp64_sweep", {}).get("iters")
+        src = "measured by the plain sweep in this run"
+        if iters is None:
+            iters, src = recorded_iters(args.workload)
+            src = "recorded: %s" % src
+        if iters:
+            spi, done, cores = cpu_sample(m, args.cpu_sample_iters)
+            line["cpu_baseline"] = cpu_baseline_obj(spi, done, cores, iters, src, nsys)
+            line["cpu_baseline"]["extrapolated"] = True
     s.close()
     if rank == 0:
         print(json.dumps(line))

@@ -234,6 +234,45 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega,
                     const aphid_sweep_opts *opts, aphid_z *x_out,
                     aphid_info *info);
 
+/* A source of the batched sweep, as gen_rhs forms it (src/aphid.f90:534-743):
+ *   oper_mode 2: x-polarised MT plane-wave source, a sheet current on every
+ *                x-edge of node layer k = 2 (src/aphid.f90:590-603);
+ *   oper_mode 3: y-polarised MT source on the y-edges of layer 2 (:607-619);
+ *   oper_mode 5: a dipole list (:638-741): ndip dipoles, 2 chars each in
+ *                dip_dir ("+X" ... "-Z") and their 1-based tail-end nodes,
+ *                3 ints each, in dip_ijk; invalid or out-of-range dipoles are
+ *                skipped as the reference skips them.
+ * The MPI farm's aphid_mpi.input chooses between the two kinds: MT sweeps
+ * run modes 2 and 3 per frequency, CS sweeps one mode-5 list per dipole
+ * array (src/aphid_parallel.f90:75-103). */
+typedef struct {
+  int oper_mode;
+  int ndip;
+  const char *dip_dir;
+  const int *dip_ijk;
+} aphid_source;
+
+/* aphid_gpu_sweep with sources of any of the kinds above: system s solves
+ * for source srcs[source_of_system[s]] at omega[s].  aphid_gpu_sweep is this
+ * call with every source a dipole list. */
+int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega,
+                            const int *source_of_system, int nsrc,
+                            const aphid_source *srcs, const aphid_z *x0,
+                            const aphid_sweep_opts *opts, aphid_z *x_out,
+                            aphid_info *info);
+
+/* Receiver gather after a sweep: E and H = B / mu0 at nrec mesh nodes for
+ * every system of the last sweep, without moving the solutions to the host.
+ * The node values are dump_fields' EM_grid interpolation
+ * (src/aphid.f90:2012-2165): E is the mean of the two edges through the node
+ * along each axis (E = -i omega (A - grad Phi), gen_fields
+ * src/aphid.f90:2225-2250), B the mean of the four faces around the node
+ * (B = curl A, :2191-2216).  rec_ijk: 1-based node indices, 3 ints per
+ * receiver, each in 2..n-1 as EM_grid's nodes are.  E, H (either may be
+ * NULL): [nsys][nrec][3] values (x, y, z components). */
+int aphid_gpu_sweep_receivers(aphid_ctx *ctx, int nrec, const int *rec_ijk,
+                              aphid_z *E, aphid_z *H);
+
 /* z-planes per work item of the complex64 pass in use (the autotuner's
  * choice unless aphid_opts.plane_kz fixed it); 0 before the first mixed
  * sweep. */
@@ -279,10 +318,11 @@ int aphid_gpu_sweep_apply(aphid_ctx *ctx, const aphid_z *x, aphid_z *y);
  * file-scope device array of about 400 KB, held by every GPU that loads the
  * library until the process exits; meshes larger than
  * APHID_NOALLOC_MAX_NODES nodes per axis are rejected with APHID_ERR_BADARG.
- * All calls share that array: calls that overlap on the GPU race on it.  The
- * first call on a device looks the array up, so make it before any stream
- * capture.  Runs on `stream` (a cudaStream_t, NULL = legacy default) and
- * returns after the launch. */
+ * All calls share that array: calls that overlap on the GPU race on it.  Each
+ * call looks up the array's address in the current context; the first call
+ * on a device also loads the library's kernels there, so make it before any
+ * stream capture.  Runs on `stream` (a cudaStream_t, NULL = legacy default)
+ * and returns after the launch. */
 #define APHID_NOALLOC_MAX_NODES 1024
 #define APHID_NOALLOC_MAX_SLOTS 16384
 int aphid_gpu_inprod_eps_noalloc(int nx, int ny, int nz,

@@ -185,6 +185,81 @@ def test_sweep_rejects_bad_input(solver):
         solver.sweep([1.0], [[("+X", 6, 6, 4)]], [3])
 
 
+def em_grid(g, B, E, i, j, k):
+    """dump_fields' EM_grid node values (src/aphid.f90:2012-2165) from the
+    oracle's gen_fields arrays at 0-based node (i, j, k): E the mean of the
+    two edges along each axis, B the mean of the four faces around the node
+    (over the four distinct By faces)"""
+    nx, ny, nz = g.dims
+    oy = (nx - 1) * ny * nz
+    oz = oy + nx * (ny - 1) * nz
+    ex = E[:oy].reshape((nx - 1, ny, nz), order="F")
+    ey = E[oy:oz].reshape((nx, ny - 1, nz), order="F")
+    ez = E[oz:].reshape((nx, ny, nz - 1), order="F")
+    nbx, nby = nx * (ny - 1) * (nz - 1), (nx - 1) * ny * (nz - 1)
+    bx = B[:nbx].reshape((nx, ny - 1, nz - 1), order="F")
+    by = B[nbx:nbx + nby].reshape((nx - 1, ny, nz - 1), order="F")
+    bz = B[nbx + nby:].reshape((nx - 1, ny - 1, nz), order="F")
+    e = [0.5 * (ex[i - 1, j, k] + ex[i, j, k]), 0.5 * (ey[i, j - 1, k] + ey[i, j, k]),
+         0.5 * (ez[i, j, k - 1] + ez[i, j, k])]
+    b = [0.25 * (bx[i, j - 1, k - 1] + bx[i, j, k - 1] + bx[i, j - 1, k] + bx[i, j, k]),
+         0.25 * (by[i - 1, j, k - 1] + by[i, j, k - 1] + by[i - 1, j, k] + by[i, j, k]),
+         0.25 * (bz[i - 1, j - 1, k] + bz[i, j - 1, k] + bz[i - 1, j, k] + bz[i, j, k])]
+    return np.array(e), np.array(b) / model.MU0
+
+
+def test_receiver_gather_matches_oracle_fields(solver):
+    """aphid_gpu_sweep_receivers on a heterogeneous model, two systems:
+    the node values agree with the EM_grid interpolation of the oracle's
+    gen_fields applied to the same (fetched) solutions, to FP64 rounding;
+    receivers off the interior are refused."""
+    xn, yn, zn, sig, _ = small_model(seed=21, dims=(17, 15, 16), nair=4)
+    g = O.Grid(xn, yn, zn)
+    om = [2 * np.pi * 0.7, 2 * np.pi * 30.0]
+    solver.set_nodes(xn, yn, zn)
+    solver.set_model("R", sig)
+    X, inf = solver.sweep(om, [[("+X", 8, 7, 5)], [("+Y", 5, 5, 5), ("-Z", 9, 9, 9)]], [0, 1])
+    rec = [[2, 2, 2], [9, 8, 5], [16, 14, 15], [5, 11, 6]]
+    E, H = solver.sweep_receivers(rec)
+    for s in range(2):
+        B, Ef = O.gen_fields(g, om[s], X[s])
+        for r, (i, j, k) in enumerate(rec):
+            e, h = em_grid(g, B, Ef, i - 1, j - 1, k - 1)
+            scale_e = np.abs(Ef).max()
+            scale_h = np.abs(B).max() / model.MU0
+            assert np.abs(E[s, r] - e).max() < 1e-12 * scale_e, (s, r, E[s, r], e)
+            assert np.abs(H[s, r] - h).max() < 1e-12 * scale_h, (s, r, H[s, r], h)
+    for bad in ([1, 5, 5], [5, 5, 16], [17, 5, 5]):
+        with pytest.raises(AphidError):
+            solver.sweep_receivers([bad])
+
+
+def test_failed_allocation_leaves_no_stale_sweep_state():
+    """A sweep whose device allocation fails (an absurd batch) returns
+    APHID_ERR_NOMEM, and the post-sweep hooks then refuse the previous
+    sweep's state (APHID_ERR_STATE / BADARG) instead of launching on freed
+    buffers; the next sweep of a sane batch works again."""
+    xn, yn, zn, sig, _ = small_model(seed=5, dims=(40, 40, 40))
+    src = [[("+X", 20, 20, 4)]]
+    with Solver(graph_iters=8, plane_kz=8) as s:
+        s.set_nodes(xn, yn, zn)
+        s.set_model("R", sig)
+        _, inf = s.sweep([2 * np.pi], src, [0], fetch=False)
+        assert inf[0]["status_name"] == "converged"
+        s.sweep_time_apply(1)
+        big = 300000  # 2 x 300000 x 253 K complex128 values: terabytes
+        with pytest.raises(AphidError, match="out of device memory"):
+            s.sweep(np.full(big, 2 * np.pi), src, np.zeros(big, np.int32), fetch=False)
+        with pytest.raises(AphidError, match="call order"):
+            s.sweep_time_apply(1)
+        with pytest.raises(AphidError, match="call order"):
+            s.sweep_apply(np.zeros(s.n, np.complex128))
+        with pytest.raises(AphidError, match="bad argument"):
+            s.sweep_fetch(0)
+        X, inf = s.sweep([2 * np.pi], src, [0])
+        assert inf[0]["status_name"] == "converged" and np.isfinite(X).all()
+
+
 def test_autotuner_picks_and_caches_the_slab_depth(tmp_path, monkeypatch):
     """plane_kz = 0: the pass depth is timed on the device per (mesh, batch,
     model kind), kept in the process and in APHID_TUNE_CACHE; a fixed
@@ -203,8 +278,9 @@ def test_autotuner_picks_and_caches_the_slab_depth(tmp_path, monkeypatch):
         X2, _ = s.sweep(w, src, [0, 0])
         assert s.sweep_plane_kz() == kz          # cached, not retuned
         assert np.array_equal(X1, X2)            # same depth, same bits
-    lines = cache.read_text().split()
-    assert lines[-6:] == [str(v) for v in (18, 17, 26, 2, 0, kz)]
+    rec = cache.read_text().split()
+    sms, name_hash = _device_identity()
+    assert rec[-8:] == [str(v) for v in (18, 17, 26, 2, 0, sms, name_hash, kz)]
     with Solver(graph_iters=8, plane_kz=8) as s:
         s.set_nodes(xn, yn, zn)
         s.set_model("R", sig)
@@ -213,6 +289,35 @@ def test_autotuner_picks_and_caches_the_slab_depth(tmp_path, monkeypatch):
     for a, b, ia, ib in zip(X1, X3, i1, i3):
         assert ia["status_name"] == ib["status_name"] == "converged"
         assert relerr(a, b) < 1e-6
+
+
+def _device_identity():
+    """(multiprocessor count, FNV-1a hash of the device name) of device 0, as
+    the tune cache records them"""
+    import torch
+    p = torch.cuda.get_device_properties(0)
+    h = 2166136261
+    for c in p.name.encode():
+        h = ((h ^ c) * 16777619) & 0xFFFFFFFF
+    return p.multi_processor_count, h & 0x7FFFFFFF
+
+
+def test_tune_cache_file_is_per_device_and_skips_torn_records(tmp_path, monkeypatch):
+    """A record for another device (other SM count) is not used, a torn line
+    is skipped, and this device's record is taken without retuning."""
+    sms, name_hash = _device_identity()
+    cache = tmp_path / "tune.txt"
+    cache.write_text("15 14 13 1 0 %d %d 16\n15 14 13 1 0 %d\n15 14 13 1 0 %d %d 6\n"
+                     % (sms + 4, name_hash, sms, sms, name_hash))
+    monkeypatch.setenv("APHID_TUNE_CACHE", str(cache))
+    xn, yn, zn, sig, _ = small_model(seed=12, dims=(15, 14, 13))
+    with Solver(graph_iters=8) as s:
+        s.set_nodes(xn, yn, zn)
+        s.set_model("R", sig)
+        _, inf = s.sweep([2 * np.pi], [[("+X", 7, 7, 4)]], [0])
+        assert inf[0]["status_name"] == "converged"
+        assert s.sweep_plane_kz() == 6
+    assert len(cache.read_text().splitlines()) == 3  # taken from the file: nothing appended
 
 
 @pytest.mark.parametrize("precision,tol_norm,tol_row", [("mixed", 1e-6, 1e-5), ("fused64", 1e-13, 1e-11)])
