@@ -91,6 +91,7 @@ def load():
     L.aphid_gpu_inprod_dev.argtypes = [P, P, P, P, P]
     L.aphid_gpu_inprod_eps_noalloc.argtypes = [C.c_int] * 3 + [P] * 11
     L.aphid_gpu_set_model.argtypes = [P, C.c_char, P, P]
+    L.aphid_gpu_set_model_cole_cole.argtypes = [P, P, P, P, P]
     L.aphid_gpu_sweep.argtypes = [P, C.c_int, P, P, C.c_int, P, C.c_char_p, P, P,
                                   C.POINTER(SweepOpts), P, P]
     L.aphid_gpu_sweep_sources.argtypes = [P, C.c_int, P, P, C.c_int, P, P, C.POINTER(SweepOpts), P, P]
@@ -310,6 +311,23 @@ class Solver:
             self._h, csig_flag.encode(),
             self._model[0].ctypes.data if self._model[0] is not None else None,
             self._model[1].ctypes.data if self._model[1] is not None else None), "set_model")
+
+    def set_model_cole_cole(self, sig_re, eta, tau, cee):
+        """Cole-Cole cell model (csig_flag 'D'): real(4) cell arrays sigma,
+        eta, tau, c; each sweep forms the averaged sigma-hat of every
+        frequency on the device."""
+        nx, ny, nz = self.dims
+        nc = (nx - 1) * (ny - 1) * (nz - 1)
+        arrs = []
+        for a in (sig_re, eta, tau, cee):
+            a = np.asarray(a, dtype=np.float32)
+            a = np.ascontiguousarray(a.ravel(order="F") if a.ndim == 3 else a)
+            if a.size != nc:
+                raise ValueError("cell array must have %d values" % nc)
+            arrs.append(a)
+        self._model = arrs
+        self._check(self.lib.aphid_gpu_set_model_cole_cole(self._h, *[a.ctypes.data for a in arrs]),
+                    "set_model_cole_cole")
 
     def sweep(self, omegas, sources, source_of_system=None, x0=None, precision="auto",
               target=1e-8, max_it=20000, inner_tol=0.0, max_outer=0, stall_window=0, fetch=True,

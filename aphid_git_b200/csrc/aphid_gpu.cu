@@ -73,14 +73,18 @@ struct aphid_ctx {
   double *d_sig64 = nullptr, *d_epsr64 = nullptr;  // FP64 node-layout copies (complex128 pass)
   float *d_cells = nullptr;  // staging of the real(4) cell arrays (set_model)
   long long cells_cap = 0;
+  int model_copies = 0;      // model arrays held: 1 (shared by all systems) or one per system (Cole-Cole)
+  float *d_cc = nullptr;     // Cole-Cole cell arrays sigma, eta, tau, c ([4][ncell], real(4))
   // sweep state
   int sw_nsys = 0;           // systems the buffers hold
   bool sw_f32_ok = false;    // complex64 vectors allocated
   double2 *sw_f64 = nullptr; // [2][nsys][n]: x64, b
-  float2 *sw_f32 = nullptr;  // [8][nsys][4][N]: 2 sets of q^ v^ p^, then d^ x^ (node layout)
+  float2 *sw_f32 = nullptr;  // [2 sets][nsys][q^ v^], [ring+1][nsys] p^, [nsys] d^; each [4][N] (node layout)
+  int sw_ring = 0;           // R of the complex64 buffers (pending updates between two flushes)
   float4 *sw_ax32 = nullptr; // FP32 axis tables of the complex64 pass
-  double2 *sw_w64 = nullptr; // [8][nsys64][4][N]: the complex128 pass's q^ v^ p^ (2 sets), d^, x^
+  double2 *sw_w64 = nullptr; // the complex128 pass's q^ v^ (2 sets), p^ ring, d^: the sw_f32 layout
   int sw_nsys64 = 0;         // systems sw_w64 holds
+  int sw_ring64 = 0;         // its R
   double4 *sw_ax64 = nullptr; // FP64 axis tables of the complex128 pass
   int *sw_work = nullptr;    // [2] work counter of the persistent pass, then [order]
   int num_sms = 148;         // multiprocessors of the device
@@ -328,6 +332,7 @@ int aphid_gpu_destroy(aphid_ctx *ctx) {
   cudaFree(ctx->d_sig64);
   cudaFree(ctx->d_epsr64);
   cudaFree(ctx->d_cells);
+  cudaFree(ctx->d_cc);
   if (ctx->h_done) cudaFreeHost(ctx->h_done);
   if (ctx->h_ndone) cudaFreeHost(ctx->h_ndone);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -371,6 +376,9 @@ int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz, const double *dx,
   ctx->d_epsr32 = nullptr;
   ctx->d_sig64 = nullptr;
   ctx->d_epsr64 = nullptr;
+  cudaFree(ctx->d_cc);
+  ctx->d_cc = nullptr;
+  ctx->model_copies = 0;
   ctx->has_mesh = false;
   ctx->has_model = false;
 
@@ -731,63 +739,38 @@ int encode_map(aphid_ctx *ctx, CUtensorMap *m, CUtensorMapDataType type, int ran
   return APHID_OK;
 }
 
-// q^, v^, p^ of both buffer sets: 5-D (i, j, k, vector x component,
-// set x system) over 8-byte elements; one box = 20 x 18 nodes of one z-plane,
-// all three vectors and four components
-int vector_maps(aphid_ctx *ctx) {
+// Inner vectors of a sweep as TMA tensors over 8-byte elements (a complex64
+// value, or the real or imaginary half of a complex128 one: xs = 1 or 2 per
+// node along i).  w: q^ and v^ of both buffer sets, 5-D (i, j, k, vector x
+// component = 8, set x system), one box = 20 x 18 nodes of one z-plane, both
+// vectors and four components; p: the p^ ring, 5-D (i, j, k, component, slot
+// x system), one box = the same nodes, four components.
+int inner_maps(aphid_ctx *ctx, CUtensorMap *w, CUtensorMap *p, void *base, int nsys, int ring, int xs) {
   const NodeLayout &L = ctx->nl;
-  const cuuint64_t dims[5] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 12,
-                              2 * (cuuint64_t)ctx->sw_nsys};
-  const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * 8, (cuuint64_t)L.nxp * ctx->ny * 8, (cuuint64_t)L.N * 8,
-                                 (cuuint64_t)L.N * 96};
-  const cuuint32_t box[5] = {kPW, kPH, 1, 12, 1};
-  int rc = encode_map(ctx, &ctx->maps.w, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32, dims, strides, box);
+  const cuuint64_t es = 8 * (cuuint64_t)xs;  // bytes per node and component
+  const cuuint64_t dims[5] = {(cuuint64_t)xs * L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 8,
+                              2 * (cuuint64_t)nsys};
+  const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * es, (cuuint64_t)L.nxp * ctx->ny * es, (cuuint64_t)L.N * es,
+                                 (cuuint64_t)L.N * 8 * es};
+  const cuuint32_t box[5] = {(cuuint32_t)(xs * kPW), kPH, 1, 8, 1};
+  int rc = encode_map(ctx, w, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, base, dims, strides, box);
   if (rc) return rc;
-  // d^, x^: 5-D (i, j, k, component, system); one box = the 16 x 16 tile of
-  // one z-plane, four components
-  const size_t v32 = (size_t)ctx->sw_nsys * 4 * L.N;
-  const cuuint64_t odims[5] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4,
-                               (cuuint64_t)ctx->sw_nsys};
-  const cuuint64_t ostrides[4] = {(cuuint64_t)L.nxp * 8, (cuuint64_t)L.nxp * ctx->ny * 8, (cuuint64_t)L.N * 8,
-                                  (cuuint64_t)L.N * 32};
-  const cuuint32_t obox[5] = {kPTI, kPTJ, 1, 4, 1};
-  if ((rc = encode_map(ctx, &ctx->maps.dd, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + 6 * v32, odims,
-                       ostrides, obox)))
-    return rc;
-  return encode_map(ctx, &ctx->maps.xx, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_f32 + 7 * v32, odims, ostrides,
-                    obox);
-}
-
-// complex128 q^, v^, p^ of both sets: 5-D (real/imaginary doubles along i,
-// j, k, vector x component, set x system) over 8-byte elements; one box = the
-// same 20 x 18 nodes of one z-plane as the complex64 map
-int vector_maps64(aphid_ctx *ctx) {
-  const NodeLayout &L = ctx->nl;
-  const cuuint64_t dims[5] = {2 * (cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 12,
-                              2 * (cuuint64_t)ctx->sw_nsys64};
-  const cuuint64_t strides[4] = {(cuuint64_t)L.nxp * 16, (cuuint64_t)L.nxp * ctx->ny * 16, (cuuint64_t)L.N * 16,
-                                 (cuuint64_t)L.N * 192};
-  const cuuint32_t box[5] = {2 * kPW, kPH, 1, 12, 1};
-  int rc = encode_map(ctx, &ctx->maps.w64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64, dims, strides, box);
-  if (rc) return rc;
-  // d^, x^: (2 nxp, ny, nz, component, system); one box = the 16 x 16 tile
-  const size_t v64 = (size_t)ctx->sw_nsys64 * 4 * L.N;
-  const cuuint64_t odims[5] = {2 * (cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4,
-                               (cuuint64_t)ctx->sw_nsys64};
-  const cuuint64_t ostrides[4] = {(cuuint64_t)L.nxp * 16, (cuuint64_t)L.nxp * ctx->ny * 16, (cuuint64_t)L.N * 16,
-                                  (cuuint64_t)L.N * 64};
-  const cuuint32_t obox[5] = {2 * kPTI, kPTJ, 1, 4, 1};
-  if ((rc = encode_map(ctx, &ctx->maps.dd64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64 + 6 * v64, odims, ostrides,
-                       obox)))
-    return rc;
-  return encode_map(ctx, &ctx->maps.xx64, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, ctx->sw_w64 + 7 * v64, odims, ostrides,
-                    obox);
+  const size_t vec = (size_t)nsys * 4 * L.N * xs;  // 8-byte elements per vector of all systems
+  const cuuint64_t pdims[5] = {(cuuint64_t)xs * L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4,
+                               (cuuint64_t)(ring + 1) * nsys};
+  const cuuint64_t pstrides[4] = {(cuuint64_t)L.nxp * es, (cuuint64_t)L.nxp * ctx->ny * es, (cuuint64_t)L.N * es,
+                                  (cuuint64_t)L.N * 4 * es};
+  const cuuint32_t pbox[5] = {(cuuint32_t)(xs * kPW), kPH, 1, 4, 1};
+  return encode_map(ctx, p, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, (double *)base + 4 * vec, pdims, pstrides, pbox);
 }
 
 // sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18
+// (one box holds the four components of one model copy; copies follow each
+// other along the component dimension)
 int model_maps(aphid_ctx *ctx) {
   const NodeLayout &L = ctx->nl;
-  const cuuint64_t dims[4] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 4};
+  const cuuint64_t dims[4] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz,
+                              4 * (cuuint64_t)std::max(1, ctx->model_copies)};
   const cuuint64_t strides[3] = {(cuuint64_t)L.nxp * 4, (cuuint64_t)L.nxp * ctx->ny * 4, (cuuint64_t)L.N * 4};
   const cuuint32_t box[4] = {kKW, kPH, 1, 4};
   int rc = encode_map(ctx, &ctx->maps.sig, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->d_sig32, dims, strides, box);
@@ -811,6 +794,8 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   D.epsr = ctx->d_epsr;
   D.sig32 = ctx->d_sig32;
   D.epsr32 = ctx->d_epsr32;
+  D.mref = ctx->csig == 'D' ? ctx->n : 0;
+  D.mnode = ctx->csig == 'D' ? 4 * ctx->nl.N : 0;
   D.L = ctx->nl;
   D.err = ctx->sw_err;
   D.tmix = 1.f;
@@ -820,15 +805,17 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
   if (ctx->sw_f32_ok) {
     D.W = ctx->sw_f32;
-    D.dd = ctx->sw_f32 + 6 * v32;
-    D.xx = ctx->sw_f32 + 7 * v32;
+    D.P = ctx->sw_f32 + 4 * v32;
+    D.dd = ctx->sw_f32 + (5 + ctx->sw_ring) * v32;
+    D.ring = ctx->sw_ring;
     D.ax32 = ctx->sw_ax32;
   }
   if (ctx->sw_w64) {
     const size_t v64 = (size_t)ctx->sw_nsys64 * 4 * ctx->nl.N;
     D.W64 = ctx->sw_w64;
-    D.dd64 = ctx->sw_w64 + 6 * v64;
-    D.xx64 = ctx->sw_w64 + 7 * v64;
+    D.P64 = ctx->sw_w64 + 4 * v64;
+    D.dd64 = ctx->sw_w64 + (5 + ctx->sw_ring64) * v64;
+    D.ring64 = ctx->sw_ring64;
     D.ax64 = ctx->sw_ax64;
   }
   D.sig64 = ctx->d_sig64;
@@ -884,6 +871,25 @@ int plane_tiles(aphid_ctx *ctx, int kz) {
   return APHID_OK;
 }
 
+// The inner buffers of a batched sweep hold 6 + R vectors per system (q^ v^ of
+// two sets, R + 1 p^ slots, d^).  R, the number of passes between two flushes
+// of the pending solution updates, is the largest of 8, 4, 2, 1 that divides
+// the passes of a graph round and leaves `reserve` bytes of device memory
+// free; bytes_per_vec is one vector of all the systems.  0 when not even
+// R = 1 fits.
+int choose_ring(const aphid_ctx *ctx, size_t bytes_per_vec, size_t reserve) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    fr = 0;
+  }
+  for (int r : {8, 4, 2, 1}) {
+    if (ctx->graph_iters % r) continue;
+    if ((6 + (size_t)r) * bytes_per_vec + reserve <= fr) return r;
+  }
+  return 0;
+}
+
 int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
   const bool grow = nsys > ctx->sw_nsys;
   if (grow || (mixed && !ctx->sw_f32_ok)) {
@@ -930,13 +936,15 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
   }
   if (mixed && !ctx->sw_f32_ok) {
     const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
-    if (cudaMalloc(&ctx->sw_f32, 8 * v32 * sizeof(float2)) != cudaSuccess) {
+    const int ring = choose_ring(ctx, v32 * sizeof(float2), (size_t)2 << 30);
+    if (!ring || cudaMalloc(&ctx->sw_f32, (6 + ring) * v32 * sizeof(float2)) != cudaSuccess) {
       cudaGetLastError();
       ctx->sw_f32 = nullptr;
       return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex64 vectors failed");
     }
+    ctx->sw_ring = ring;
     // pads and components that do not exist stay zero for good
-    CK(cudaMemset(ctx->sw_f32, 0, 8 * v32 * sizeof(float2)));
+    CK(cudaMemset(ctx->sw_f32, 0, (6 + ring) * v32 * sizeof(float2)));
     if (!ctx->sw_ax32) {
       CK(cudaMalloc(&ctx->sw_ax32, 2 * (size_t)(ctx->nx + ctx->ny + ctx->nz) * sizeof(float4)));
       const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));
@@ -945,7 +953,7 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     }
     if (!ctx->sw_err) CK(cudaMalloc(&ctx->sw_err, sizeof(int)));
     ctx->sw_f32_ok = true;
-    int rc = vector_maps(ctx);
+    int rc = inner_maps(ctx, &ctx->maps.w, &ctx->maps.p, ctx->sw_f32, ctx->sw_nsys, ring, 1);
     if (rc) return rc;
   }
   return APHID_OK;
@@ -960,12 +968,14 @@ int sweep_alloc64(aphid_ctx *ctx, int k) {
   ctx->sw_w64 = nullptr;
   ctx->sw_nsys64 = 0;
   const size_t v64 = (size_t)k * 4 * ctx->nl.N;
-  if (cudaMalloc(&ctx->sw_w64, 8 * v64 * sizeof(double2)) != cudaSuccess) {
+  const int ring = choose_ring(ctx, v64 * sizeof(double2), (size_t)1 << 30);
+  if (!ring || cudaMalloc(&ctx->sw_w64, (6 + ring) * v64 * sizeof(double2)) != cudaSuccess) {
     cudaGetLastError();
     ctx->sw_w64 = nullptr;
     return fail(ctx, APHID_ERR_NOMEM, "sweep: device allocation of the complex128 inner vectors failed");
   }
-  CK(cudaMemsetAsync(ctx->sw_w64, 0, 8 * v64 * sizeof(double2), ctx->stream));
+  ctx->sw_ring64 = ring;
+  CK(cudaMemsetAsync(ctx->sw_w64, 0, (6 + ring) * v64 * sizeof(double2), ctx->stream));
   if (!ctx->sw_ax64) {
     CK(cudaMalloc(&ctx->sw_ax64, 2 * (size_t)(ctx->nx + ctx->ny + ctx->nz) * sizeof(double4)));
     const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));
@@ -974,7 +984,7 @@ int sweep_alloc64(aphid_ctx *ctx, int k) {
   }
   if (!ctx->sw_err) CK(cudaMalloc(&ctx->sw_err, sizeof(int)));
   ctx->sw_nsys64 = k;
-  return vector_maps64(ctx);
+  return inner_maps(ctx, &ctx->maps.w64, &ctx->maps.p64, ctx->sw_w64, k, ring, 2);
 }
 
 // Sources (gen_rhs, src/aphid.f90:534-743) as sparse (index, value) lists
@@ -1057,10 +1067,11 @@ int pass_attrs(aphid_ctx *ctx) {
   return APHID_OK;
 }
 
-// persistent: one block per SM
+// persistent: PassShm<EPS>::blocks resident blocks per SM
 void launch_pass(aphid_ctx *ctx, const SweepDev &D, bool timing) {
   const long long items = D.tp.count() * D.nsys;
-  const unsigned sp = (unsigned)std::min<long long>(items, (long long)ctx->num_sms);
+  const int per_sm = D.epsr32 ? PassShm<true>::blocks : PassShm<false>::blocks;
+  const unsigned sp = (unsigned)std::min<long long>(items, (long long)per_sm * ctx->num_sms);
   const size_t shm = pass_shm(D);
   if (D.epsr32) {
     if (timing)
@@ -1092,17 +1103,23 @@ void launch_pass64(aphid_ctx *ctx, const SweepDev &D, bool timing) {
   }
 }
 
+// One graph round: flush the pending solution updates (this ends the inner
+// cycles that stopped in the last round), the outer step (FP64 residual and
+// restart) of the systems between cycles, graph_iters passes with a flush
+// after every R of them, and the true-residual monitor.
 template <typename T>
 void sweep_round_t(aphid_ctx *ctx, const SweepDev &D) {
   const unsigned ps = (unsigned)(D.bps * D.nsys);
   const unsigned st = (unsigned)(D.t.count() * D.nsys);
-  k_sw_xupd<T><<<ps, kStreamThreads, 0, ctx->stream>>>(D);
+  const int ring = sizeof(T) == sizeof(double2) ? D.ring64 : D.ring;
+  k_sw_dxupd<T, false><<<ps, kStreamThreads, 0, ctx->stream>>>(D);
   k_sw_resid<T><<<st, kOpThreads, 0, ctx->stream>>>(D);
   for (int it = 0; it < ctx->graph_iters; it++) {
     if (sizeof(T) == sizeof(double2))
       launch_pass64(ctx, D, false);
     else
       launch_pass(ctx, D, false);
+    if ((it + 1) % ring == 0) k_sw_dxupd<T, false><<<ps, kStreamThreads, 0, ctx->stream>>>(D);
   }
   k_sw_check<T><<<st, kOpThreads, 0, ctx->stream>>>(D);
 }
@@ -1264,10 +1281,15 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
 }
 
 // per-system state of a batched sweep at its start
-SweepSys sweep_sys_init(double omega, const aphid_sweep_opts *opts, bool fused, bool escalate, int max_it) {
+// k^2 = (-ka eps-bar, kb sigma-bar): models R, C, I have sigma-hat = sigma +
+// i omega eps0 eps_r, so ka = omega^2 mu0 eps0; Cole-Cole (D) keeps the real
+// and imaginary averages of its sigma-hat in sigma-bar and eps-bar, so
+// k^2 = i omega mu0 (Re + i Im) gives ka = kb = omega mu0
+SweepSys sweep_sys_init(double omega, const aphid_sweep_opts *opts, bool fused, bool escalate, int max_it,
+                        char csig = 'R') {
   SweepSys S{};
   S.omega = omega;
-  S.ka = omega * omega * kMu0 * kEps0;
+  S.ka = csig == 'D' ? omega * kMu0 : omega * omega * kMu0 * kEps0;
   S.kb = omega * kMu0;
   S.target = opts->target;
   S.max_it = max_it;
@@ -1310,7 +1332,7 @@ int run_batched(aphid_ctx *ctx, const SweepDev &D, bool fused, std::vector<Sweep
   CK(cudaGetLastError());
   nlaunch += 1;
   if ((rc = sweep_graph(ctx, D, fused))) return rc;
-  const long long per_round = 3 + (long long)ctx->graph_iters;
+  const long long per_round = 3 + (long long)ctx->graph_iters + ctx->graph_iters / (fused ? D.ring64 : D.ring);
   const long long max_rounds = (long long)std::max(1, max_it) / ctx->graph_iters + 2LL * (hs[0].max_outer + 2);
   for (long long round = 0;; round++) {
     CK(cudaMemcpyAsync(ctx->h_ndone, ctx->sw_ndone, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1328,16 +1350,30 @@ int run_batched(aphid_ctx *ctx, const SweepDev &D, bool fused, std::vector<Sweep
   return APHID_OK;
 }
 
-// exchange the x and b slots of systems p and q (tmp: 2 n complex128)
+// exchange the x and b slots of systems p and q, and their model arrays
+// when every system has its own (Cole-Cole) (tmp: 2 n complex128)
 int swap_systems(aphid_ctx *ctx, int p, int q, double2 *tmp) {
   if (p == q) return APHID_OK;
   const size_t n = (size_t)ctx->n, bytes = n * sizeof(double2), cap = (size_t)ctx->sw_nsys * n;
-  double2 *base[2] = {ctx->sw_f64, ctx->sw_f64 + cap};
-  for (int v = 0; v < 2; v++) {
-    double2 *a = base[v] + (size_t)p * n, *c = base[v] + (size_t)q * n;
-    CK(cudaMemcpyAsync(tmp, a, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(a, c, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(c, tmp, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  struct Blk {
+    void *base;
+    size_t bytes;
+  };
+  std::vector<Blk> blks = {{ctx->sw_f64, bytes}, {ctx->sw_f64 + cap, bytes}};
+  if (ctx->csig == 'D') {
+    const size_t nn = 4 * (size_t)ctx->nl.N;
+    blks.push_back({ctx->d_sig, n * sizeof(double)});
+    blks.push_back({ctx->d_epsr, n * sizeof(double)});
+    blks.push_back({ctx->d_sig32, nn * sizeof(float)});
+    blks.push_back({ctx->d_epsr32, nn * sizeof(float)});
+    blks.push_back({ctx->d_sig64, nn * sizeof(double)});
+    blks.push_back({ctx->d_epsr64, nn * sizeof(double)});
+  }
+  for (const Blk &b : blks) {
+    char *a = (char *)b.base + (size_t)p * b.bytes, *c = (char *)b.base + (size_t)q * b.bytes;
+    CK(cudaMemcpyAsync(tmp, a, b.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(a, c, b.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(c, tmp, b.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   }
   return APHID_OK;
 }
@@ -1368,8 +1404,11 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
     cudaFree(tmp);
     return cuda_fail(ctx, me, "cudaMemGetInfo");
   }
-  const size_t per = 8 * 4 * (size_t)ctx->nl.N * sizeof(double2) + ((size_t)1 << 26);
-  const size_t have = fr + (ctx->sw_w64 ? (size_t)ctx->sw_nsys64 * 8 * 4 * ctx->nl.N * sizeof(double2) : 0);
+  // per system: 6 + R complex128 node vectors; sized for R = 4 (sweep_alloc64
+  // picks the largest R that fits the chunk)
+  const size_t per = 10 * 4 * (size_t)ctx->nl.N * sizeof(double2) + ((size_t)1 << 26);
+  const size_t have =
+      fr + (ctx->sw_w64 ? (size_t)ctx->sw_nsys64 * (6 + ctx->sw_ring64) * 4 * ctx->nl.N * sizeof(double2) : 0);
   const int cap = (int)std::max<size_t>(1, std::min<size_t>(esc.size(), (have - std::min(have, (size_t)1 << 30)) / per));
   for (size_t c0 = 0; c0 < esc.size() && !rc; c0 += cap) {
     const int k = (int)std::min<size_t>(cap, esc.size() - c0);
@@ -1394,7 +1433,8 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
     std::vector<SweepSys> h2(k);
     for (int q = 0; q < k; q++) {
       const int s = esc[c0 + q];
-      h2[q] = sweep_sys_init(omega[s], opts, true, false, std::max(1, opts->max_it - out[s].inner_iters));
+      h2[q] = sweep_sys_init(omega[s], opts, true, false, std::max(1, opts->max_it - out[s].inner_iters),
+                             ctx->csig);
     }
     SweepDev D2 = sweep_dev(ctx, k);
     rc = run_batched(ctx, D2, true, h2, opts->max_it, nlaunch);
@@ -1423,6 +1463,107 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
   ctx->sw_nsys64 = 0;
   if (!rc && se != cudaSuccess) rc = cuda_fail(ctx, se, "sweep (escalated systems)");
   return rc;
+}
+
+// (Re)allocate the model arrays for `copies` model copies: sigma-bar (and
+// eps-bar when eps) in FP64 reference layout and in FP32 and FP64 node layout.
+int alloc_model(aphid_ctx *ctx, int copies, bool eps) {
+  const size_t n = (size_t)ctx->n * copies, nn = 4 * (size_t)ctx->nl.N * copies;
+  if (ctx->model_copies != copies) {
+    cudaFree(ctx->d_sig);
+    cudaFree(ctx->d_sig32);
+    cudaFree(ctx->d_sig64);
+    cudaFree(ctx->d_epsr);
+    cudaFree(ctx->d_epsr32);
+    cudaFree(ctx->d_epsr64);
+    ctx->d_sig = ctx->d_epsr = ctx->d_sig64 = ctx->d_epsr64 = nullptr;
+    ctx->d_sig32 = ctx->d_epsr32 = nullptr;
+    ctx->model_copies = 0;
+  }
+  auto get = [&](void **p, size_t bytes) -> int {
+    if (*p) return APHID_OK;
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      *p = nullptr;
+      return fail(ctx, APHID_ERR_NOMEM, "device allocation of the model arrays failed");
+    }
+    return APHID_OK;
+  };
+  int rc;
+  if ((rc = get((void **)&ctx->d_sig, n * sizeof(double))) || (rc = get((void **)&ctx->d_sig32, nn * sizeof(float))) ||
+      (rc = get((void **)&ctx->d_sig64, nn * sizeof(double))))
+    return rc;
+  if (eps) {
+    if ((rc = get((void **)&ctx->d_epsr, n * sizeof(double))) ||
+        (rc = get((void **)&ctx->d_epsr32, nn * sizeof(float))) ||
+        (rc = get((void **)&ctx->d_epsr64, nn * sizeof(double))))
+      return rc;
+  } else {
+    cudaFree(ctx->d_epsr);
+    cudaFree(ctx->d_epsr32);
+    cudaFree(ctx->d_epsr64);
+    ctx->d_epsr = ctx->d_epsr64 = nullptr;
+    ctx->d_epsr32 = nullptr;
+  }
+  ctx->model_copies = copies;
+  return APHID_OK;
+}
+
+int ensure_cells(aphid_ctx *ctx, long long count) {
+  if (ctx->cells_cap >= count) return APHID_OK;
+  cudaFree(ctx->d_cells);
+  ctx->d_cells = nullptr;
+  ctx->cells_cap = 0;
+  CK(cudaMalloc(&ctx->d_cells, count * sizeof(float)));
+  ctx->cells_cap = count;
+  return APHID_OK;
+}
+
+// node-layout FP32 and FP64 copies of model copy c from its reference-layout
+// averages (zeros where a component does not exist)
+int model_to_node(aphid_ctx *ctx, int c) {
+  const dim3 grid = node_grid(ctx);
+  const size_t nn = 4 * (size_t)ctx->nl.N, n = (size_t)ctx->n;
+  const double *src[2] = {ctx->d_sig + c * n, ctx->d_epsr ? ctx->d_epsr + c * n : nullptr};
+  float *d32[2] = {ctx->d_sig32 + c * nn, ctx->d_epsr32 ? ctx->d_epsr32 + c * nn : nullptr};
+  double *d64[2] = {ctx->d_sig64 + c * nn, ctx->d_epsr64 ? ctx->d_epsr64 + c * nn : nullptr};
+  for (int q = 0; q < 2; q++) {
+    if (!src[q]) continue;
+    CK(cudaMemsetAsync(d32[q], 0, nn * sizeof(float), ctx->stream));
+    k_sw_to_node<float><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, src[q], d32[q]);
+    CK(cudaMemsetAsync(d64[q], 0, nn * sizeof(double), ctx->stream));
+    k_sw_to_node<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, src[q], d64[q]);
+  }
+  CK(cudaGetLastError());
+  return APHID_OK;
+}
+
+// Cole-Cole: one model copy per system of the sweep, sigma-hat(omega_s)
+// averaged as gen_k2_*grid averages it (real part into sigma-bar, imaginary
+// into eps-bar)
+int build_cole_cole(aphid_ctx *ctx, int nsys, const double *omega) {
+  int rc;
+  if ((rc = alloc_model(ctx, nsys, true))) return rc;
+  const long long ncell = (long long)(ctx->nx - 1) * (ctx->ny - 1) * (ctx->nz - 1);
+  double *cell = nullptr;
+  if (cudaMalloc(&cell, 2 * ncell * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, APHID_ERR_NOMEM, "sweep: no memory for the Cole-Cole cell values");
+  }
+  const dim3 grid = node_grid(ctx);
+  const float *cc = ctx->d_cc;
+  for (int s = 0; s < nsys && !rc; s++) {
+    k_cc_cells<<<(unsigned)std::min<long long>((ncell + 255) / 256, 148 * 16), 256, 0, ctx->stream>>>(
+        ncell, cc, cc + ncell, cc + 2 * ncell, cc + 3 * ncell, omega[s], cell, cell + ncell);
+    k_sw_avg<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, cell, ctx->d_sig + (size_t)s * ctx->n);
+    k_sw_avg<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, cell + ncell, ctx->d_epsr + (size_t)s * ctx->n);
+    rc = model_to_node(ctx, s);
+  }
+  const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(cell);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "Cole-Cole model");
+  return model_maps(ctx);
 }
 
 template <typename T>
@@ -1467,7 +1608,7 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
   if (rc) return rc;
   if (csig_flag == 'D')
     return fail(ctx, APHID_ERR_BADARG,
-                "Cole-Cole (D) is not linear in omega: use aphid_gpu_gen_k2 + aphid_gpu_qmr per frequency");
+                "Cole-Cole (D) needs four cell arrays: use aphid_gpu_set_model_cole_cole");
   if (csig_flag != 'R' && csig_flag != 'C' && csig_flag != 'I')
     return fail(ctx, APHID_ERR_BADARG, "csig_flag must be R, C or I");
   if ((csig_flag != 'I' && !sig_re) || (csig_flag != 'R' && !eps_rel))
@@ -1477,52 +1618,45 @@ int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re, con
   if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
   ctx->sw_gexec = nullptr;
   ctx->has_model = false;
-  if (!ctx->d_sig) CK(cudaMalloc(&ctx->d_sig, ctx->n * sizeof(double)));
-  if (!ctx->d_sig32) CK(cudaMalloc(&ctx->d_sig32, 4 * ctx->nl.N * sizeof(float)));
-  if (!ctx->d_sig64) CK(cudaMalloc(&ctx->d_sig64, 4 * ctx->nl.N * sizeof(double)));
-  if (csig_flag != 'R') {
-    if (!ctx->d_epsr) CK(cudaMalloc(&ctx->d_epsr, ctx->n * sizeof(double)));
-    if (!ctx->d_epsr32) CK(cudaMalloc(&ctx->d_epsr32, 4 * ctx->nl.N * sizeof(float)));
-    if (!ctx->d_epsr64) CK(cudaMalloc(&ctx->d_epsr64, 4 * ctx->nl.N * sizeof(double)));
-  } else {
-    cudaFree(ctx->d_epsr);
-    cudaFree(ctx->d_epsr32);
-    cudaFree(ctx->d_epsr64);
-    ctx->d_epsr = nullptr;
-    ctx->d_epsr32 = nullptr;
-    ctx->d_epsr64 = nullptr;
-  }
-  if (ctx->cells_cap < ncell) {
-    cudaFree(ctx->d_cells);
-    ctx->d_cells = nullptr;
-    ctx->cells_cap = 0;
-    CK(cudaMalloc(&ctx->d_cells, ncell * sizeof(float)));
-    ctx->cells_cap = ncell;
-  }
+  if ((rc = alloc_model(ctx, 1, csig_flag != 'R'))) return rc;
+  if ((rc = ensure_cells(ctx, ncell))) return rc;
   float *cells = ctx->d_cells;
   const dim3 grid = node_grid(ctx);
   if (csig_flag == 'I') {
     CK(cudaMemsetAsync(ctx->d_sig, 0, ctx->n * sizeof(double), ctx->stream));
   } else {
     CK(cudaMemcpyAsync(cells, sig_re, ncell * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    k_sw_avg<<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_sig);
+    k_sw_avg<float><<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_sig);
   }
   if (csig_flag != 'R') {
     CK(cudaMemcpyAsync(cells, eps_rel, ncell * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    k_sw_avg<<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_epsr);
-    CK(cudaMemsetAsync(ctx->d_epsr32, 0, 4 * ctx->nl.N * sizeof(float), ctx->stream));
-    k_sw_to_node<float><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_epsr, ctx->d_epsr32);
-    CK(cudaMemsetAsync(ctx->d_epsr64, 0, 4 * ctx->nl.N * sizeof(double), ctx->stream));
-    k_sw_to_node<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_epsr, ctx->d_epsr64);
+    k_sw_avg<float><<<grid, 128, 0, ctx->stream>>>(ctx->g, cells, ctx->d_epsr);
   }
-  CK(cudaMemsetAsync(ctx->d_sig32, 0, 4 * ctx->nl.N * sizeof(float), ctx->stream));
-  k_sw_to_node<float><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_sig, ctx->d_sig32);
-  CK(cudaMemsetAsync(ctx->d_sig64, 0, 4 * ctx->nl.N * sizeof(double), ctx->stream));
-  k_sw_to_node<double><<<grid, 128, 0, ctx->stream>>>(ctx->g, ctx->nl, ctx->d_sig, ctx->d_sig64);
-  CK(cudaGetLastError());
+  if ((rc = model_to_node(ctx, 0))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
-  if ((rc = model_maps(ctx))) return rc;
   ctx->csig = csig_flag;
+  if ((rc = model_maps(ctx))) return rc;
+  ctx->has_model = true;
+  return APHID_OK;
+}
+
+int aphid_gpu_set_model_cole_cole(aphid_ctx *ctx, const float *sig_re, const float *eta, const float *tau,
+                                  const float *cee) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!sig_re || !eta || !tau || !cee) return fail(ctx, APHID_ERR_BADARG, "missing Cole-Cole cell array");
+  const long long ncell = (long long)(ctx->nx - 1) * (ctx->ny - 1) * (ctx->nz - 1);
+  if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+  ctx->sw_gexec = nullptr;
+  ctx->has_model = false;
+  cudaFree(ctx->d_cc);
+  ctx->d_cc = nullptr;
+  CK(cudaMalloc(&ctx->d_cc, 4 * ncell * sizeof(float)));
+  const float *src[4] = {sig_re, eta, tau, cee};
+  for (int q = 0; q < 4; q++)
+    CK(cudaMemcpyAsync(ctx->d_cc + q * ncell, src[q], ncell * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->csig = 'D';
   ctx->has_model = true;
   return APHID_OK;
 }
@@ -1581,6 +1715,12 @@ int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega, const
   if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
   if (fused && (rc = sweep_alloc64(ctx, nsys))) return rc;
   if ((rc = ensure_work(ctx))) return rc;
+  if (ctx->csig == 'D') {
+    // the model follows the frequencies: one averaged sigma-hat per system
+    if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+    ctx->sw_gexec = nullptr;
+    if ((rc = build_cole_cole(ctx, nsys, omega))) return rc;
+  }
   if (mixed || fused) {
     if (ctx->plane_kz > 0) {
       if (ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) && (rc = plane_tiles(ctx, ctx->plane_kz)))
@@ -1620,7 +1760,8 @@ int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega, const
     CK(cudaMemsetAsync(x64, 0, vec * sizeof(double2), ctx->stream));
 
   std::vector<SweepSys> hs(nsys);
-  for (int s = 0; s < nsys; s++) hs[s] = sweep_sys_init(omega[s], opts, fused, prec == APHID_PREC_AUTO, opts->max_it);
+  for (int s = 0; s < nsys; s++)
+    hs[s] = sweep_sys_init(omega[s], opts, fused, prec == APHID_PREC_AUTO, opts->max_it, ctx->csig);
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   long long nlaunch = 0;
   std::vector<aphid_info> out(nsys);
@@ -1638,7 +1779,9 @@ int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega, const
     // the reference's own algorithm, one system at a time, on resident data
     double2 *k2 = wv(ctx, W_K2), *dg = wv(ctx, W_INV);
     for (int s = 0; s < nsys; s++) {
-      k_sw_k2vec<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_sig, ctx->d_epsr, hs[s].ka,
+      const long long mo = ctx->csig == 'D' ? (long long)s * ctx->n : 0;
+      k_sw_k2vec<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_sig + mo,
+                                                                 ctx->d_epsr ? ctx->d_epsr + mo : nullptr, hs[s].ka,
                                                                  hs[s].kb, k2);
       k_gen_diag<<<node_grid(ctx), 128, 0, ctx->stream>>>(ctx->g, k2, dg);
       CK(cudaMemcpyAsync(wv(ctx, W_B), b + (size_t)s * ctx->n, ctx->n * sizeof(double2),

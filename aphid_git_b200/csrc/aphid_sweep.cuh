@@ -31,19 +31,27 @@
 // v^_{n-1}, p^_{n-1} with halos and forms, per node,
 //   vt_n = q^_{n-1} - beta_{n-1} v^_{n-1},  v^_n = vt_n / rho_n,
 //   p^_n = v^_n - k1_n p^_{n-1}   (k1_n = rho_n delta_n / epsilon_{n-1}),
-// applies the stencil, q^_n = D^-1 K p^_n, applies the lagged update
-// d^_{n-1} = eta_{n-1} p^_{n-1} + kappa_{n-1} d^_{n-2}, x^ += d^_{n-1}, and
-// stores v^_n, p^_n, q^_n into the other buffer set (the halo reads of the
-// next pass must not see this pass's writes).  It reduces epsilon_n =
-// p~_n^T q~_n and the six inner products of v~_n and q~_n from which
-// rho_{n+1} = ||q~_n - beta_n v~_n|| and delta_{n+1} = v~_{n+1}^T v~_{n+1}
-// follow without another pass over the vectors (beta_n is not known until
-// the pass has finished).  The last block to finish runs the scalar
-// recurrences.  The expansions are accumulated in FP64 from per-node FP32
-// products; the cycle restarts from the FP64 residual when they lose accuracy
-// (see kCancel and kDrift).  No residual vectors are kept: the stop test uses
-// the quasi-residual tau_n = ||r~_0|| prod sqrt(theta_i c_i), which a
-// complex128 true-residual monitor checks once per graph round.
+// applies the stencil, q^_n = D^-1 K p^_n, and stores v^_n, q^_n into the
+// other (q, v) buffer set (the halo reads of the next pass must not see this
+// pass's writes) and p^_n into the next slot of a ring of R+1 p^ buffers.  It
+// reduces epsilon_n = p~_n^T q~_n and the six inner products of v~_n and q~_n
+// from which rho_{n+1} = ||q~_n - beta_n v~_n|| and delta_{n+1} =
+// v~_{n+1}^T v~_{n+1} follow without another pass over the vectors (beta_n is
+// not known until the pass has finished).  The last block to finish runs the
+// scalar recurrences and appends (eta_n, kappa_n, ring slot of p^_n) to the
+// system's pending-update list.  The expansions are accumulated in FP64 from
+// per-node FP32 products; the cycle restarts from the FP64 residual when they
+// lose accuracy (see kCancel and kDrift).  No residual vectors are kept: the
+// stop test uses the quasi-residual tau_n = ||r~_0|| prod sqrt(theta_i c_i),
+// which a complex128 true-residual monitor checks once per graph round.
+//
+// The solution update d^_n = eta_n p^_n + kappa_n d^_{n-1}, x += d^_n is not
+// in the pass: after every R passes a streaming kernel (k_sw_dxupd) applies
+// the pending updates of each system from the ring, accumulating the R
+// increments in FP64 straight into the reference-layout solution x.  The pass
+// then moves 48 B per unknown instead of 80 B (q^ v^ p^ read and written; d^
+// and the solution move once per R iterations, (R + 1) x 8 + 32 B), and it
+// keeps no d^ staging in shared memory.
 //
 // Every system has a phase (OUTER -> INNER -> OUTER ... -> DONE);
 // every block first reads its system's phase and returns when the kernel does
@@ -56,7 +64,7 @@
 namespace aphid {
 
 enum { PH_OUTER = 0, PH_INNER = 2, PH_DONE = 3 };
-enum { CNT_RESID = 0, CNT_PASS = 2, CNT_BNORM = 4, CNT_CHECK = 5, CNT_KINDS = 6 };
+enum { CNT_RESID = 0, CNT_PASS = 2, CNT_BNORM = 4, CNT_CHECK = 5, CNT_DX = 6, CNT_KINDS = 7 };
 constexpr int kParts = 12;  // partial sums per slot and system
 
 // An inner cycle ends when the true residual, checked once per graph round,
@@ -95,19 +103,24 @@ constexpr int kStallWindow = 400;
 // Heterogeneous land models stay above 1e-5.
 constexpr double kDeltaFloor = 1e-6;
 constexpr int kStEscalated = 4;
+// longest pending-update list (the p^ ring has up to kMaxRing + 1 slots)
+constexpr int kMaxRing = 8;
 
 struct SweepSys {
   double omega, ka, kb;  // k^2 = (-ka * eps-bar, kb * sigma-bar)
   double rho_n, rho_np, c_n, c_nm, theta_n, theta_nm, kap, tau, tau0;
   double2 eps, del, beta, eta, k1;
   double vscale;             // 1 / rho_n
-  double2 eta_pend;          // pending lagged update d = eta p + kap d
-  double kap_pend;
+  double2 eta_h[kMaxRing];   // pending solution updates d = eta p + kap d, x += d,
+  double kap_h[kMaxRing];    //   in order, p^ from ring slot slot_h
+  int slot_h[kMaxRing];
+  int npend;                 // entries of the pending list
+  int pslot;                 // ring slot of the last pass's p^
   double bnorm, rnorm, inner_tol, target, rt0;
   double ratio_min, mon_rn;  // true-residual monitor of the running inner cycle
   int phase, has_inner, inner_it, total_it, outer_it, max_it, max_outer, status;
-  int checks, pending;
-  int cur;                   // buffer set holding q^, v^, p^ of the last pass
+  int checks;
+  int cur;                   // buffer set holding q^, v^ of the last pass
   int restarts;              // inner cycles ended by kCancel / kDrift / a stall
   double tau_win;            // tau at the start of the current stall window
   int win_it;                // inner iteration at which that window started
@@ -140,9 +153,15 @@ struct SweepDev {
   const double *sig;     // sigma-bar per unknown (FP64, reference layout)
   const double *epsr;    // eps-bar per unknown, or null (= 1)
   const float *sig32, *epsr32;  // the same, FP32, node layout [4][N]
+  // per-system model arrays (Cole-Cole: sigma-hat depends on omega): system s
+  // reads sig + s mref and the node-layout arrays at + s mnode; 0 when all
+  // systems share one model
+  long long mref, mnode;
   const float4 *ax32;    // per axis: [n] (n4, n5, dc, 1/dc), then [n] (e2, e3, d, 1/d) of edge m
-  float2 *W;             // [2 sets][nsys][q^, v^, p^][4][N] complex64
-  float2 *dd, *xx;              // [nsys][4][N]: d^, x^
+  float2 *W;             // [2 sets][nsys][q^, v^][4][N] complex64
+  float2 *P;             // [ring + 1 slots][nsys][4][N]: p^
+  float2 *dd;            // [nsys][4][N]: d^
+  int ring;              // R: pending updates between two k_sw_dxupd launches
   double2 *x64, *b;              // [nsys][n] complex128, reference layout
   SweepSys *sys;
   double *part;                  // [nsys][slots][kParts]
@@ -153,20 +172,28 @@ struct SweepDev {
   int *work;                     // [2]: next work item, blocks finished (complex64 pass)
   const int *order;              // plane tiles in the order the pass takes them
   // complex128 inner storage (k_sw_pass64): same layouts, double2
-  double2 *W64, *dd64, *xx64;
+  double2 *W64, *P64, *dd64;
+  int ring64;
   const double *sig64, *epsr64;  // sigma-bar / eps-bar, FP64, node layout [4][N]
   const double4 *ax64;           // the axis tables of ax32 in FP64
 };
 
+// q^ (vec 0) or v^ (vec 1) of buffer set `set`; p^ of ring slot `slot`
 __device__ __forceinline__ float2 *wvec(const SweepDev &D, int set, int sys, int vec) {
-  return D.W + ((long long)(set * D.nsys + sys) * 3 + vec) * 4 * D.L.N;
+  return D.W + ((long long)(set * D.nsys + sys) * 2 + vec) * 4 * D.L.N;
+}
+__device__ __forceinline__ float2 *pvec(const SweepDev &D, int slot, int sys) {
+  return D.P + (long long)(slot * D.nsys + sys) * 4 * D.L.N;
 }
 __device__ __forceinline__ double4 ldg4(const double4 *p) {
   const double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
   return make_double4(a.x, a.y, b.x, b.y);
 }
 __device__ __forceinline__ double2 *wvec64(const SweepDev &D, int set, int sys, int vec) {
-  return D.W64 + ((long long)(set * D.nsys + sys) * 3 + vec) * 4 * D.L.N;
+  return D.W64 + ((long long)(set * D.nsys + sys) * 2 + vec) * 4 * D.L.N;
+}
+__device__ __forceinline__ double2 *pvec64(const SweepDev &D, int slot, int sys) {
+  return D.P64 + (long long)(slot * D.nsys + sys) * 4 * D.L.N;
 }
 __device__ __forceinline__ long long nd_of(const SweepDev &D, int i, int j, int k) {
   return i + (long long)D.L.nxp * (j + (long long)D.g.ny * k);
@@ -376,7 +403,7 @@ __device__ __forceinline__ void rowsN(const GridDev &g, int i, int j, int k, con
 }
 
 // complex128 accessors of the outer passes
-struct K2Ref64 {  // k^2 from the FP64 averages (reference layout)
+struct K2Ref64 {  // k^2 from the FP64 averages of one system (reference layout)
   GridDev g;
   const double *__restrict__ sig, *__restrict__ epsr;
   double ka, kb;
@@ -423,7 +450,8 @@ __device__ __forceinline__ void mark_done(const SweepDev &D, SweepSys *S, int st
 // sigma-bar / eps-bar per unknown: the area- and volume-weighted cell
 // averages of gen_k2_*grid before the factor i omega mu0, boundary values
 // from the clamped interior index (src/aphid.f90:1289-1535).
-static __global__ void k_sw_avg(GridDev g, const float *__restrict__ cell, double *__restrict__ out) {
+template <typename CT>
+static __global__ void k_sw_avg(GridDev g, const CT *__restrict__ cell, double *__restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= g.nx) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz, cx = nx - 1, cy = ny - 1;
@@ -466,6 +494,27 @@ static __global__ void k_sw_avg(GridDev g, const float *__restrict__ cell, doubl
     s += S(ii, jj, kk - 1) * (dxi * dyj * dzkm);
     s += S(ii - 1, jj, kk - 1) * (dxim * dyj * dzkm);
     out[ixp(g, i, j, k)] = s / ((dxim + dxi) * (dyjm + dyj) * (dzkm + dzk));
+  }
+}
+
+// Cole-Cole cell conductivity at one frequency (read_mesh model D,
+// src/aphid.f90:410-435): sigma-hat = sigma (1 - eta / (1 + (i omega tau)^c))
+// from the real(4) cell arrays, in FP64; (i omega tau)^c on the principal
+// branch, (omega tau)^c (cos(pi c / 2) + i sin(pi c / 2)).  Real and
+// imaginary parts go to re[] and im[].
+static __global__ void k_cc_cells(long long ncell, const float *__restrict__ sig, const float *__restrict__ eta,
+                                  const float *__restrict__ tau, const float *__restrict__ cee, double omega,
+                                  double *__restrict__ re, double *__restrict__ im) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell;
+       t += (long long)gridDim.x * blockDim.x) {
+    const double s = sig[t], e = eta[t], ta = tau[t], c = cee[t];
+    double sn, cs;
+    sincospi(0.5 * c, &sn, &cs);
+    const double mag = ta > 0.0 ? pow(omega * ta, c) : 0.0;
+    const double2 den = make_double2(1.0 + mag * cs, mag * sn);
+    const double2 f = cdiv(make_double2(e, 0.0), den);
+    re[t] = s * (1.0 - f.x);
+    im[t] = -s * f.y;
   }
 }
 
@@ -560,8 +609,9 @@ __device__ __forceinline__ void node_diag32(const SweepDev &D, const SweepSys *S
   const int nx = D.g.nx, ny = D.g.ny, nz = D.g.nz;
   const long long N = D.L.N, plane = (long long)D.L.nxp * ny, nd = nd_of(D, i, j, k);
   const float4 *AX = D.ax32, *AY = D.ax32 + 2 * nx, *AZ = D.ax32 + 2 * (nx + ny);
-  auto sg = [&](int c, long long q) { return __ldg(D.sig32 + c * N + q); };
-  auto ep = [&](int c, long long q) { return D.epsr32 ? __ldg(D.epsr32 + c * N + q) : 1.f; };
+  const long long mo = (S - D.sys) * D.mnode;
+  auto sg = [&](int c, long long q) { return __ldg(D.sig32 + mo + c * N + q); };
+  auto ep = [&](int c, long long q) { return D.epsr32 ? __ldg(D.epsr32 + mo + c * N + q) : 1.f; };
   const bool pin = i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1;
   jacobi32(__ldg(AX + i), __ldg(AX + nx + i), __ldg(AY + j), __ldg(AY + ny + j), __ldg(AZ + k), __ldg(AZ + nz + k),
            sg(0, nd), sg(1, nd), sg(2, nd), sg(3, nd), pin ? sg(0, nd - 1) : 0.f, pin ? sg(1, nd - D.L.nxp) : 0.f,
@@ -575,8 +625,9 @@ __device__ __forceinline__ void node_diag64(const SweepDev &D, const SweepSys *S
   const int nx = D.g.nx, ny = D.g.ny, nz = D.g.nz;
   const long long N = D.L.N, plane = (long long)D.L.nxp * ny, nd = nd_of(D, i, j, k);
   const double4 *AX = D.ax64, *AY = D.ax64 + 2 * nx, *AZ = D.ax64 + 2 * (nx + ny);
-  auto sg = [&](int c, long long q) { return __ldg(D.sig64 + c * N + q); };
-  auto ep = [&](int c, long long q) { return D.epsr64 ? __ldg(D.epsr64 + c * N + q) : 1.0; };
+  const long long mo = (S - D.sys) * D.mnode;
+  auto sg = [&](int c, long long q) { return __ldg(D.sig64 + mo + c * N + q); };
+  auto ep = [&](int c, long long q) { return D.epsr64 ? __ldg(D.epsr64 + mo + c * N + q) : 1.0; };
   const bool pin = i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1;
   jacobi64(ldg4(AX + i), ldg4(AX + nx + i), ldg4(AY + j), ldg4(AY + ny + j), ldg4(AZ + k), ldg4(AZ + nz + k),
            sg(0, nd), sg(1, nd), sg(2, nd), sg(3, nd), pin ? sg(0, nd - 1) : 0.0, pin ? sg(1, nd - D.L.nxp) : 0.0,
@@ -592,8 +643,9 @@ template <> struct Inner<float2> {
   static __device__ __forceinline__ float2 *vec(const SweepDev &D, int set, int sys, int v) {
     return wvec(D, set, sys, v);
   }
+  static __device__ __forceinline__ float2 *pv(const SweepDev &D, int slot, int sys) { return pvec(D, slot, sys); }
   static __device__ __forceinline__ float2 *dd(const SweepDev &D) { return D.dd; }
-  static __device__ __forceinline__ float2 *xx(const SweepDev &D) { return D.xx; }
+  static __device__ __forceinline__ int ring(const SweepDev &D) { return D.ring; }
   static __device__ __forceinline__ void diag(const SweepDev &D, const SweepSys *S, int i, int j, int k,
                                               float2 dg[4]) {
     node_diag32(D, S, i, j, k, dg);
@@ -605,8 +657,9 @@ template <> struct Inner<double2> {
   static __device__ __forceinline__ double2 *vec(const SweepDev &D, int set, int sys, int v) {
     return wvec64(D, set, sys, v);
   }
+  static __device__ __forceinline__ double2 *pv(const SweepDev &D, int slot, int sys) { return pvec64(D, slot, sys); }
   static __device__ __forceinline__ double2 *dd(const SweepDev &D) { return D.dd64; }
-  static __device__ __forceinline__ double2 *xx(const SweepDev &D) { return D.xx64; }
+  static __device__ __forceinline__ int ring(const SweepDev &D) { return D.ring64; }
   static __device__ __forceinline__ void diag(const SweepDev &D, const SweepSys *S, int i, int j, int k,
                                               double2 dg[4]) {
     node_diag64(D, S, i, j, k, dg);
@@ -622,7 +675,7 @@ static __global__ void k_sw_apply_in(SweepDev D, const double2 *__restrict__ x) 
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= D.g.nx) return;
   const int cur = D.sys->cur;
-  T *Q = Inner<T>::vec(D, cur, 0, 0), *V = Inner<T>::vec(D, cur, 0, 1), *P = Inner<T>::vec(D, cur, 0, 2);
+  T *Q = Inner<T>::vec(D, cur, 0, 0), *V = Inner<T>::vec(D, cur, 0, 1), *P = Inner<T>::pv(D, D.sys->pslot, 0);
   const long long nd = nd_of(D, i, j, k);
   const T zero = Inner<T>::from_d(make_double2(0.0, 0.0));
 #pragma unroll
@@ -648,24 +701,47 @@ static __global__ void k_sw_apply_out(SweepDev D, double2 *__restrict__ y) {
 }
 
 // ------------------------------------------------------------ outer step
-// O1: x += x^ (+ the pending lagged update), FP64 accumulation of the inner
-// correction into the reference-layout solution at the end of an inner
-// cycle.  During a cycle (once per graph round) the same kernel moves x^ into
-// x and zeroes it, leaving the pending update pending: x^ then only ever
-// holds the last round's increments, so its complex64 rounding no longer
-// sets the floor of the cycle (about 8x lower on the test meshes).
-template <typename T>
-static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
+// The deferred solution update (k_sw_dxupd): for every system with pending
+// updates n1 .. nk (eta_j, kappa_j and the ring slot of p^_j, appended by the
+// passes), per unknown
+//   d^ <- eta_j p^_j + kappa_j d^,  dx += d^   (j = n1 .. nk, in order),
+// then x += dx in FP64 (reference layout) and the list is emptied.  d^ stays
+// in the inner precision T, the increments of the R passes are summed in
+// FP64.  This is the update of src/aphid_qmr.f90:347-354 (d = eta p + kappa
+// d, x = x + d), applied R iterations at a time: the graph launches it after
+// every R passes, at the start of each round (ending a cycle before its
+// residual) and before the true-residual monitor.
+// TIMING: the same loads, stores and arithmetic with eta = 0, kappa = 1 over
+// R ring slots and x += 0 dx (tmix = 0), leaving d^ and x as they were.
+__device__ __forceinline__ float2 dx_link(float2 e, float2 p, float k, float2 d) {  // e p + k d
+  return make_float2(fmaf(e.x, p.x, fmaf(-e.y, p.y, k * d.x)), fmaf(e.x, p.y, fmaf(e.y, p.x, k * d.y)));
+}
+__device__ __forceinline__ double2 dx_link(double2 e, double2 p, double k, double2 d) {
+  return make_double2(fma(e.x, p.x, fma(-e.y, p.y, k * d.x)), fma(e.x, p.y, fma(e.y, p.x, k * d.y)));
+}
+template <typename T, bool TIMING>
+static __global__ void __launch_bounds__(kStreamThreads) k_sw_dxupd(SweepDev D) {
   const int sys = blockIdx.x % D.nsys, chunk = blockIdx.x / D.nsys;
-  const SweepSys *S = D.sys + sys;
-  const bool flush = S->phase == PH_INNER;
-  if (!flush && (S->phase != PH_OUTER || !S->has_inner)) return;
-  const long long vb = (long long)sys * 4 * D.L.N;
-  const bool pend = !flush && S->pending != 0;
-  const double2 eta = S->eta_pend;
-  const double kap = S->kap_pend;
-  const T *P = Inner<T>::vec(D, S->cur, sys, 2), *dd = Inner<T>::dd(D) + vb;
-  T *xx = Inner<T>::xx(D) + vb;
+  SweepSys *S = D.sys + sys;
+  using R = typename Inner<T>::R;
+  const int ring = Inner<T>::ring(D);
+  __shared__ int s_np;
+  __shared__ T s_eta[kMaxRing];
+  __shared__ R s_kap[kMaxRing];
+  __shared__ const T *s_p[kMaxRing];
+  if (threadIdx.x == 0) s_np = TIMING ? ring : S->npend;
+  __syncthreads();
+  const int np = s_np;
+  if (np == 0) return;
+  if (threadIdx.x < np) {
+    const int q = threadIdx.x;
+    s_eta[q] = TIMING ? Inner<T>::from_d(make_double2(0.0, 0.0)) : Inner<T>::from_d(S->eta_h[q]);
+    s_kap[q] = TIMING ? (R)1 : (R)S->kap_h[q];
+    s_p[q] = Inner<T>::pv(D, TIMING ? (S->pslot + 1 + q) % (ring + 1) : S->slot_h[q], sys);
+  }
+  __syncthreads();
+  const double mix = TIMING ? (double)D.tmix : 1.0;
+  T *dd = Inner<T>::dd(D) + (long long)sys * 4 * D.L.N;
   const GridDev &g = D.g;
   const long long plane = (long long)D.L.nxp * g.ny;
   double2 *x64 = D.x64 + (long long)sys * D.n;
@@ -679,11 +755,26 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_xupd(SweepDev D) {
     for (int c = 0; c < 4; c++) {
       if (!exists(g, c, i, j, k)) continue;
       const long long t = c * D.L.N + nd;
-      double2 xt = to_d(xx[t]);
-      if (pend) xt = cadd(xt, cadd(cmul(eta, to_d(P[t])), rmul(kap, to_d(dd[t]))));
+      T d = dd[t];
+      double2 dx = make_double2(0.0, 0.0);
+      for (int q = 0; q < np; q++) {
+        d = dx_link(s_eta[q], __ldg(s_p[q] + t), s_kap[q], d);
+        dx = cadd(dx, to_d(d));
+      }
+      dd[t] = d;
       const long long rt = ref_of(g, c, i, j, k);
-      x64[rt] = cadd(x64[rt], xt);
-      if (flush) xx[t] = Inner<T>::from_d(make_double2(0.0, 0.0));
+      x64[rt] = make_double2(fma(mix, dx.x, x64[rt].x), fma(mix, dx.y, x64[rt].y));
+    }
+  }
+  // the last block of this system empties its pending list
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned *cnt = D.cnt + CNT_DX * D.nsys + sys;
+    if (atomicAdd(cnt, 1u) == (unsigned)D.bps - 1) {
+      if (!TIMING) S->npend = 0;
+      *cnt = 0;
+      __threadfence();
     }
   }
 }
@@ -699,11 +790,11 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
   Vals<4> a{{0.0, 0.0, 0.0, 0.0}};
   if (i < D.g.nx && j < D.g.ny) {
     const XRef64 L{D.g, D.x64 + (long long)sys * D.n, nullptr, D.L.nxp, D.L.N};
-    const K2Ref64 K{D.g, D.sig, D.epsr, S->ka, S->kb};
+    const K2Ref64 K{D.g, D.sig + sys * D.mref, D.epsr ? D.epsr + sys * D.mref : nullptr, S->ka, S->kb};
     const double2 *b = D.b + (long long)sys * D.n;
     const long long vb = (long long)sys * 4 * D.L.N;
     T *Q = Inner<T>::vec(D, S->cur, sys, 0), *V = Inner<T>::vec(D, S->cur, sys, 1),
-      *P = Inner<T>::vec(D, S->cur, sys, 2), *dd = Inner<T>::dd(D), *xx = Inner<T>::xx(D);
+      *P = Inner<T>::pv(D, S->pslot, sys), *dd = Inner<T>::dd(D);
     using R = typename Inner<T>::R;
     const T zero = Inner<T>::from_d(make_double2(0.0, 0.0));
     for (int k = k0; k < k1; k++) {
@@ -733,7 +824,6 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
         V[t] = zero;
         P[t] = zero;
         dd[vb + t] = zero;
-        xx[vb + t] = zero;
       }
     }
   }
@@ -746,7 +836,7 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
     if (threadIdx.x == 0) {
       S->rnorm = sqrt(tot.v[0]);
       S->has_inner = 0;
-      S->pending = 0;
+      S->npend = 0;  // flushed by k_sw_dxupd before this step
       if (!isfinite(S->rnorm)) {
         mark_done(D, S, 3);
       } else if (S->rnorm < S->target * S->bnorm) {
@@ -786,12 +876,12 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
   }
 }
 
-// Monitor: the true residual of the running iterate, ||b - K (x + x^)|| in
-// complex128 (x^ lags one update), once per graph round once the cycle is
-// near its end (see kMonitorLevel).  Ends the inner
+// Monitor: the true residual of the running iterate, ||b - K x|| in
+// complex128 (x as k_sw_dxupd left it, every update applied), once per graph
+// round once the cycle is near its end (see kMonitorLevel).  Ends the inner
 // cycle on convergence or on stagnation of the complex64 recurrence (see
-// kStagnation); the next round's outer step folds x^ into x and restarts
-// from the FP64 residual.
+// kStagnation); the next round's outer step restarts from the FP64
+// residual.
 template <typename T>
 static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
   const int sys = blockIdx.x % D.nsys;
@@ -803,9 +893,8 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
   sweep_tile(D, tile, i, j, k0, k1);
   Vals<1> a{{0.0}};
   if (i < D.g.nx && j < D.g.ny) {
-    const long long vb = (long long)sys * 4 * D.L.N;
-    const XRefT<T> L{D.g, D.x64 + (long long)sys * D.n, Inner<T>::xx(D) + vb, D.L.nxp, D.L.N};
-    const K2Ref64 K{D.g, D.sig, D.epsr, S->ka, S->kb};
+    const XRef64 L{D.g, D.x64 + (long long)sys * D.n, nullptr, D.L.nxp, D.L.N};
+    const K2Ref64 K{D.g, D.sig + sys * D.mref, D.epsr ? D.epsr + sys * D.mref : nullptr, S->ka, S->kb};
     const double2 *b = D.b + (long long)sys * D.n;
     for (int k = k0; k < k1; k++) {
       double2 o[4];
@@ -876,27 +965,30 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 
 // tensor maps of the pass (kernel parameter, __grid_constant__)
 struct PassMaps {
-  CUtensorMap w;         // 5-D: (nxp, ny, nz, vector x component = 12, set x system), 8-byte elements
+  CUtensorMap w;         // 5-D: (nxp, ny, nz, vector x component = 8 (q^ v^), set x system), 8-byte elements
+  CUtensorMap p;         // 5-D: (nxp, ny, nz, component, ring slot x system), 8-byte elements
   CUtensorMap sig, eps;  // 4-D: (nxp, ny, nz, component), FP32
-  CUtensorMap dd, xx;    // 5-D: (nxp, ny, nz, component, system), 8-byte elements
-  CUtensorMap w64;       // complex128 q^ v^ p^: 5-D (2 nxp, ny, nz, 12, set x system), 8-byte elements
-  CUtensorMap dd64, xx64;  // complex128 d^, x^: 5-D (2 nxp, ny, nz, component, system), 8-byte elements
+  CUtensorMap w64;       // complex128 q^ v^: 5-D (2 nxp, ny, nz, 8, set x system), 8-byte elements
+  CUtensorMap p64;       // complex128 p^ ring: 5-D (2 nxp, ny, nz, 4, slot x system), 8-byte elements
 };
 
-constexpr int kStages = 3;                       // load ring depth of the pass
 constexpr unsigned kVecPlane = kPN * 8u;         // one component of one vector, one staged plane
 constexpr unsigned kRawBytes = 12u * kVecPlane;  // q^, v^, p^ with halo, four components each
 constexpr unsigned kSigBytes = 4u * kKN * 4u;    // sigma-bar with halo, four components
-constexpr unsigned kOwnBytes = 4u * kPThreads * 8u;  // d^ or x^ of the tile, no halo
 constexpr unsigned kUBytes = 4u * kVecPlane;     // u of one plane
-// shared memory of the pass: kStages load stages (q^ v^ p^ d^ x^ of plane
-// m+1 and sigma-bar [eps-bar] of plane m), two u planes, the mbarriers
+// Shared memory and occupancy of the pass.  Model R: two load stages
+// (41.5 KB each) and two blocks per SM (16 warps, at most 128 registers per
+// thread); models C, I and D stage eps-bar too and run three stages in one
+// block per SM.  Each stage holds q^ v^ (8 components) and p^ (4) of plane
+// m+1 with halo and sigma-bar [eps-bar] of plane m; then two u planes and the
+// mbarriers.
 template <bool EPS>
 struct PassShm {
+  static constexpr int stages = EPS ? 3 : 2;
+  static constexpr int blocks = EPS ? 1 : 2;  // resident blocks per SM
   static constexpr unsigned sig = kRawBytes;
-  static constexpr unsigned own = kRawBytes + (EPS ? 2u : 1u) * kSigBytes;  // d^, then x^
-  static constexpr unsigned stage = own + 2u * kOwnBytes;
-  static constexpr size_t bytes = kStages * (size_t)stage + 2 * (size_t)kUBytes + 128;
+  static constexpr unsigned stage = kRawBytes + (EPS ? 2u : 1u) * kSigBytes;
+  static constexpr size_t bytes = stages * (size_t)stage + 2 * (size_t)kUBytes + 128;
 };
 constexpr int kWaitTries = 1 << 24;
 
@@ -983,11 +1075,11 @@ __device__ __forceinline__ float2 node_row_c(float2 f, float2 fxp, float2 fxm, f
 // Scalar step at the end of pass n (one thread): epsilon_n, beta_n,
 // rho_{n+1} and delta_{n+1} from the pipelined inner products, then theta,
 // c, eta, kappa, tau and k1 as in src/aphid_qmr.f90:324-372.
-__device__ __noinline__ void pass_scalars(SweepSys *S, const double *T) {
+__device__ __noinline__ void pass_scalars(SweepSys *S, const double *T, int ring) {
   S->cur ^= 1;
+  S->pslot = (S->pslot + 1) % (ring + 1);
   S->inner_it++;
   S->total_it++;
-  S->pending = 0;
   const double2 e = make_double2(T[0], T[1]);
   S->eps = e;
   if (!finite2(e) || zero2(e)) {  // breakdown: restart from the current x
@@ -1014,9 +1106,15 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T) {
   S->eta = cdiv(rmul(S->c_n, rmul(S->rho_n, cneg(S->eta))), rmul(S->c_nm, beta));
   S->kap = S->theta_nm * S->c_n;
   S->tau = S->tau * sqrt(S->theta_n * S->c_n);
-  S->eta_pend = S->eta;
-  S->kap_pend = S->kap;
-  S->pending = finite2(S->eta) && isfinite(S->kap);
+  // the solution update of this iteration, d = eta p^_n + kappa d, x += d, for
+  // k_sw_dxupd (the graph flushes the list before it can exceed the ring)
+  const bool update = finite2(S->eta) && isfinite(S->kap) && S->npend < kMaxRing;
+  if (update) {
+    S->eta_h[S->npend] = S->eta;
+    S->kap_h[S->npend] = S->kap;
+    S->slot_h[S->npend] = S->pslot;
+    S->npend++;
+  }
   if (exhausted) {
     S->phase = PH_OUTER;
     return;
@@ -1035,7 +1133,7 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T) {
   }
   if (stall) S->restarts++;
   if (S->escalate && sqrt(cabs2(del)) < kDeltaFloor * A3) S->escalated = 1;
-  if (S->escalated || !S->pending || !isfinite(S->tau) || !finite2(del) || zero2(del) || drift || stall ||
+  if (S->escalated || !update || !isfinite(S->tau) || !finite2(del) || zero2(del) || drift || stall ||
       S->tau < S->inner_tol * S->tau0 || S->total_it >= S->max_it) {
     S->phase = PH_OUTER;
     return;
@@ -1052,10 +1150,10 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T) {
 // takes (tile, system) work items from a counter, tiles with the most live
 // nodes first.  A 16 x 16 node tile marches along k.  Thread 0 issues, per
 // z-plane, one TMA transaction into a kStages-deep ring: q^, v^, p^ of plane
-// m+1 (all four components, 20 x 18 nodes with halo), d^ and x^ of plane m+1
-// (the tile, no halo) and sigma-bar (eps-bar) of plane m, two planes ahead
-// of their use; the kernel makes no synchronous global load in its steady
-// state.  Each thread forms u = p^_n of its own node (which also gives v^_n
+// m+1 (q^ v^ of the read set and p^ of the last ring slot, all four
+// components, 20 x 18 nodes with halo) and sigma-bar (eps-bar) of plane m,
+// kStages-1 planes ahead of their use; the kernel makes no synchronous global
+// load in its steady state.  Each thread forms u = p^_n of its own node (which also gives v^_n
 // and the stored outputs) and halo values into the u plane of the next step;
 // the z-neighbours of its own node stay in registers.  The Jacobi diagonal D
 // is formed in FP32 from the same coefficients as the rows (it is their
@@ -1063,40 +1161,25 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T) {
 // zeros, and pads and absent components are stored zeros, so zero padding
 // reproduces the reference's clamped neighbours (their coefficients are zero
 // at the boundary).
-// EPS: models C and I (eps-bar not 1).  TIMING: the same pass over resident
-// data without the phase test and the scalar step, leaving d^ and x^ as they
-// were; it flips the buffer set like an iteration does, so consecutive timing
-// launches read what the previous one wrote (the x64 solution is untouched).
+// EPS: models C, I and D (eps-bar not 1).  TIMING: the same pass over
+// resident data without the phase test and the scalar step; it flips the
+// buffer set and advances the ring like an iteration does, so consecutive
+// timing launches read what the previous one wrote (d^ and the x64 solution
+// are untouched).
+// One work item (a tile's z-slab of one system) of the complex64 pass, on
+// the mesh and buffers of D with the tensor maps M.  shm: the pass's dynamic
+// shared memory; bar, phase: its stage mbarriers and their wait parities.
 template <bool EPS, bool TIMING>
-__global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __grid_constant__ PassMaps M) {
+__device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, long long item,
+                                          unsigned char *shm, unsigned long long *bar, unsigned &phase) {
   using SH = PassShm<EPS>;
+  constexpr int kStages = SH::stages;
   constexpr unsigned kStage = SH::stage;
-  extern __shared__ __align__(128) unsigned char shm[];
-  __shared__ int s_item;
   float2 *Ub = reinterpret_cast<float2 *>(shm + kStages * kStage);  // [2][4][kPN]
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + kStages * kStage + 2 * kUBytes);
-  // TMA destinations must be 128-byte aligned: refuse to copy otherwise
-  const bool aligned = (smem_u32(shm) & 127u) == 0;
-  if (!aligned && threadIdx.x == 0) atomicExch(D.err, 2);
-  if (threadIdx.x == 0 && aligned) {
-#pragma unroll
-    for (int q = 0; q < kStages; q++) mbar_init(smem_u32(&bar[q]));
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    fence_async_smem();
-  }
-  unsigned phase = 0;  // bit q: parity of the next wait on stage q
-  const long long per_sys = D.tp.count(), total = aligned ? per_sys * D.nsys : 0;
-
-  for (;;) {
-  __syncthreads();
-  if (threadIdx.x == 0) s_item = atomicAdd(D.work, 1);
-  __syncthreads();
-  const long long item = s_item;
-  if (item >= total) break;
   const int sys = (int)(item % D.nsys);
   const long long tile = __ldg(D.order + item / D.nsys);
   SweepSys *S = D.sys + sys;
-  if (!TIMING && S->phase != PH_INNER) continue;
+  if (!TIMING && S->phase != PH_INNER) return;
 
   const GridDev &g = D.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -1111,32 +1194,20 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
   const bool live = i < nx && j < ny;
   const long long N = D.L.N, plane = (long long)D.L.nxp * ny;
   const long long ndc = i + (long long)D.L.nxp * j;  // this node within a plane
-  const int cur = S->cur;
-  const long long sb = (long long)sys * 4 * N;
+  const int cur = S->cur, pslot = S->pslot;
   float2 *__restrict__ Qw = wvec(D, cur ^ 1, sys, 0);
   float2 *__restrict__ Vw = wvec(D, cur ^ 1, sys, 1);
-  float2 *__restrict__ Pw = wvec(D, cur ^ 1, sys, 2);
-  float2 *__restrict__ dd = D.dd + sb;
-  float2 *__restrict__ xx = D.xx + sb;
-  const float *__restrict__ sig = D.sig32;
-  const float *__restrict__ eps = D.epsr32;
+  float2 *__restrict__ Pw = pvec(D, (pslot + 1) % (D.ring + 1), sys);
+  const float *__restrict__ sig = D.sig32 + sys * D.mnode;
+  const float *__restrict__ eps = D.epsr32 ? D.epsr32 + sys * D.mnode : nullptr;
+  const int msig = D.mnode ? 4 * sys : 0;  // TMA component coordinate of this system's sigma-bar
   // u = ca q^ + cb v^ + cc p^ and v = ca q^ + cb v^
   const float ca = (float)S->vscale;
   const float2 cb = to_f(rmul(-S->vscale, S->beta));
   const float2 cc = to_f(cneg(S->k1));
-  const bool pend = TIMING || S->pending != 0;
-  // timing launches rewrite d^ and x^ with their own values through the same
-  // arithmetic (eta = 0, kappa = 1, x^ += 0 d^), the zeros coming from a
-  // runtime value so that the loads and stores stay in the code
-  const float xmix = TIMING ? D.tmix : 1.f;
-  float2 eta = to_f(S->eta_pend);
-  float kap = (float)S->kap_pend;
-  if (TIMING) {
-    eta = xmix != 0.f ? eta : make_float2(0.f, 0.f);
-    kap = xmix != 0.f ? kap : 1.f;
-  }
   const float ka = (float)S->ka, kb = (float)S->kb;
-  const int wset = cur * D.nsys + sys;  // TMA coordinate of the read set
+  const int wset = cur * D.nsys + sys;    // TMA coordinate of the read (q^, v^) set
+  const int pset = pslot * D.nsys + sys;  // ... and of the p^ read
 
   // thread 0: the loads of step m into stage st
   auto issue = [&](int st, int m) {
@@ -1145,10 +1216,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
     fence_async_smem();
     mbar_expect(bb, kStage);
     tma_load5(smem_u32(base), &M.w, i0 - 2, j0 - 1, m + 1, 0, wset, bb);
-    tma_load4(smem_u32(base + SH::sig), &M.sig, i0 - 4, j0 - 1, m, 0, bb);
-    if (EPS) tma_load4(smem_u32(base + SH::sig + kSigBytes), &M.eps, i0 - 4, j0 - 1, m, 0, bb);
-    tma_load5(smem_u32(base + SH::own), &M.dd, i0, j0, m + 1, 0, sys, bb);
-    tma_load5(smem_u32(base + SH::own + kOwnBytes), &M.xx, i0, j0, m + 1, 0, sys, bb);
+    tma_load5(smem_u32(base + 8u * kVecPlane), &M.p, i0 - 2, j0 - 1, m + 1, 0, pset, bb);
+    tma_load4(smem_u32(base + SH::sig), &M.sig, i0 - 4, j0 - 1, m, msig, bb);
+    if (EPS) tma_load4(smem_u32(base + SH::sig + kSigBytes), &M.eps, i0 - 4, j0 - 1, m, msig, bb);
   };
   auto wait = [&](int st) {
     if (!mbar_wait(smem_u32(&bar[st]), (phase >> st) & 1u, kWaitTries) && threadIdx.x == 0) atomicExch(D.err, 1);
@@ -1187,24 +1257,6 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
       }
     }
   };
-  // the lagged update of the own node of plane m1: p^_{n-1}, d^, x^ from
-  // stage st
-  auto dx_step = [&](int st, int m1) {
-    if (live && m1 < k1 && pend) {
-      const float2 *R = reinterpret_cast<const float2 *>(shm + st * kStage);
-      const float2 *Dd = reinterpret_cast<const float2 *>(shm + st * kStage + SH::own);
-      const float2 *Xx = Dd + 4 * kPThreads;
-      const long long nd = ndc + m1 * plane;
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        const long long t = c * N + nd;
-        const float2 d0 = Dd[c * kPThreads + threadIdx.x], x0 = Xx[c * kPThreads + threadIdx.x];
-        const float2 dn = cfma(eta, R[(8 + c) * kPN + eo], make_float2(kap * d0.x, kap * d0.y));
-        dd[t] = dn;
-        xx[t] = make_float2(fmaf(xmix, dn.x, x0.x), fmaf(xmix, dn.y, x0.y));
-      }
-    }
-  };
   auto halo = [&](int st, float2 *Us) {
     const float2 *R = reinterpret_cast<const float2 *>(shm + st * kStage);
     float2 vt;
@@ -1222,16 +1274,18 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
   const bool hx = live && i < nx - 1, hy = live && j < ny - 1;
   const bool pxy = live && i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
 
-  // ---- prologue: step k0-1 (stage 0); steps k0, k0+1 in flight
+  // ---- prologue: step k0-1 (stage 0); the next kStages-1 steps in flight
   if (threadIdx.x == 0) {
     issue(0, k0 - 1);
     issue(1, k0);
-    if (k0 + 1 <= k1 - 1) issue(2, k0 + 1);
+#pragma unroll
+    for (int q = 2; q < kStages; q++)
+      if (k0 + q - 1 <= k1 - 1) issue(q, k0 + q - 1);
   }
 #pragma unroll
   for (int c = 0; c < 4; c++) um[c] = make_float2(0.f, 0.f);
   if (live && k0 > 0) {  // u of plane k0-1, own node: the first plane's z-neighbour
-    const float2 *Qr = wvec(D, cur, sys, 0), *Vr = wvec(D, cur, sys, 1), *Pr = wvec(D, cur, sys, 2);
+    const float2 *Qr = wvec(D, cur, sys, 0), *Vr = wvec(D, cur, sys, 1), *Pr = pvec(D, pslot, sys);
     const long long nd = ndc + (k0 - 1) * plane;
     float2 vt;
 #pragma unroll
@@ -1239,12 +1293,11 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
   }
   wait(0);
   own_step(0, k0, Ub, uc, vc);
-  dx_step(0, k0);
   halo(0, Ub);
   float s2m = reinterpret_cast<const float *>(shm + SH::sig)[2 * kKN + ck];  // sigma-bar of Az at k0-1
   float e2m = EPS ? reinterpret_cast<const float *>(shm + SH::sig + kSigBytes)[2 * kKN + ck] : 1.f;
   __syncthreads();
-  if (threadIdx.x == 0 && k0 + 2 <= k1 - 1) issue(0, k0 + 2);
+  if (threadIdx.x == 0 && k0 + kStages - 1 <= k1 - 1) issue(0, k0 + kStages - 1);
 
   double acc[kParts];
 #pragma unroll
@@ -1353,10 +1406,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
 #pragma unroll
       for (int q = 0; q < kParts; q++) acc[q] += (double)r[q];
     }
-    dx_step(st, m + 1);
     if (m + 1 < k1) halo(st, Un);
     __syncthreads();  // everyone is done with stage st and with u plane m
-    if (threadIdx.x == 0 && m + 3 <= k1 - 1) issue(st, m + 3);
+    if (threadIdx.x == 0 && m + kStages <= k1 - 1) issue(st, m + kStages);
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       um[c] = uc[c];
@@ -1377,22 +1429,98 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
   if (arrive<kParts, kPThreads>(blk, part, cnt, (unsigned)tile, nt)) {
     Vals<kParts> tot = final_reduce<kParts, kPThreads>(part, cnt, nt);
     if (threadIdx.x == 0) {
-      if (TIMING)
+      if (TIMING) {
         S->cur ^= 1;
-      else
-        pass_scalars(S, tot.v);
+        S->pslot = (S->pslot + 1) % (D.ring + 1);
+      } else {
+        pass_scalars(S, tot.v, D.ring);
+      }
     }
   }
-  }  // work items
-  // the last block out re-arms the work counter for the next launch
+}
+
+// set-up of a pass block: the stage mbarriers; false when the dynamic shared
+// memory is not 128-byte aligned (TMA destinations must be; the block then
+// takes no work and the launch reports the error)
+template <int kStages>
+__device__ __forceinline__ bool pass_block_init(unsigned char *shm, unsigned long long *bar, int *err) {
+  const bool aligned = (smem_u32(shm) & 127u) == 0;
+  if (!aligned && threadIdx.x == 0) atomicExch(err, 2);
+  if (threadIdx.x == 0 && aligned) {
+#pragma unroll
+    for (int q = 0; q < kStages; q++) mbar_init(smem_u32(&bar[q]));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    fence_async_smem();
+  }
+  return aligned;
+}
+// the last block out of a persistent launch re-arms its work counter
+__device__ __forceinline__ void pass_block_done(int *work) {
   if (threadIdx.x == 0) {
     __threadfence();
-    if (atomicAdd(D.work + 1, 1) == gridDim.x - 1) {
-      D.work[0] = 0;
-      D.work[1] = 0;
+    if (atomicAdd(work + 1, 1) == gridDim.x - 1) {
+      work[0] = 0;
+      work[1] = 0;
       __threadfence();
     }
   }
+}
+
+template <bool EPS, bool TIMING>
+__global__ void __launch_bounds__(kPThreads, PassShm<EPS>::blocks) k_sw_pass(SweepDev D,
+                                                                            const __grid_constant__ PassMaps M) {
+  using SH = PassShm<EPS>;
+  extern __shared__ __align__(128) unsigned char shm[];
+  __shared__ int s_item;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * kUBytes);
+  const bool aligned = pass_block_init<SH::stages>(shm, bar, D.err);
+  unsigned phase = 0;  // bit q: parity of the next wait on stage q
+  const long long total = aligned ? D.tp.count() * D.nsys : 0;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(D.work, 1);
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= total) break;
+    pass_item<EPS, TIMING>(D, M, item, shm, bar, phase);
+  }
+  pass_block_done(D.work);
+}
+
+// Several meshes in one persistent launch (aphid_gpu_sweep_group): the
+// complex64 passes of up to kMaxGroup sweeps, each with its own mesh, model,
+// buffers and tile order, take work items from one counter.  Items are
+// numbered mesh after mesh (first[m] .. first[m+1]-1), the larger meshes
+// first, so that the smaller ones fill the tail of the launch.
+constexpr int kMaxGroup = 8;
+struct PassGroup {
+  int n;
+  int *work;  // [2]: next item, blocks finished
+  long long first[kMaxGroup + 1];
+  SweepDev D[kMaxGroup];
+  PassMaps M[kMaxGroup];
+};
+
+template <bool EPS, bool TIMING>
+__global__ void __launch_bounds__(kPThreads, PassShm<EPS>::blocks) k_sw_pass_group(const __grid_constant__ PassGroup G) {
+  using SH = PassShm<EPS>;
+  extern __shared__ __align__(128) unsigned char shm[];
+  __shared__ int s_item;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * kUBytes);
+  const bool aligned = pass_block_init<SH::stages>(shm, bar, G.D[0].err);
+  unsigned phase = 0;
+  const long long total = aligned ? G.first[G.n] : 0;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(G.work, 1);
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= total) break;
+    int m = 0;
+    while (m + 1 < G.n && item >= G.first[m + 1]) m++;
+    pass_item<EPS, TIMING>(G.D[m], G.M[m], item - G.first[m], shm, bar, phase);
+  }
+  pass_block_done(G.work);
 }
 
 
@@ -1400,15 +1528,14 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass(SweepDev D, const __gr
 // k_sw_pass64: the fused QMR iteration of k_sw_pass with complex128 vectors,
 // FP64 coefficients (sigma-bar, eps-bar, axis tables) and FP64 arithmetic, for
 // systems on which complex64 storage cannot carry the Lanczos process (see
-// kDeltaFloor).  Same tiles, same work order, same inner products and scalar
-// step (pass_scalars); 2 TMA stages of q^ v^ p^ planes (69 KB each) and one
-// TMA buffer of the own tile's d^, x^ (32 KB), loaded a plane ahead;
-// sigma-bar is read with plain loads, prefetched into L1 a plane ahead.
+// kDeltaFloor).  Same tiles, same work order, same inner products, the same
+// p^ ring and deferred solution update (k_sw_dxupd<double2>) and scalar step
+// (pass_scalars); 2 TMA stages of q^ v^ p^ planes (69 KB each); sigma-bar is
+// read with plain loads, prefetched into L1 a plane ahead.
 constexpr int kStages64 = 2;
 constexpr unsigned kRawBytes64 = 12u * kPN * 16u;  // q^, v^, p^ with halo, four components, complex128
 constexpr unsigned kUBytes64 = 4u * kPN * 16u;
-constexpr unsigned kDXBytes64 = 2u * 4u * kPThreads * 16u;  // d^ and x^ of one plane of the own tile
-constexpr size_t kPass64Shm = kStages64 * (size_t)kRawBytes64 + 2 * (size_t)kUBytes64 + kDXBytes64 + 128;
+constexpr size_t kPass64Shm = kStages64 * (size_t)kRawBytes64 + 2 * (size_t)kUBytes64 + 128;
 
 // pull a line towards this SM's L1 ahead of its use (no register, no wait)
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
@@ -1486,19 +1613,16 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
   double2 *Ub = reinterpret_cast<double2 *>(shm + kStages64 * kStage);  // [2][4][kPN]
-  // d^ then x^ of the own tile, one plane, [4][kPThreads] each
-  const double2 *DX = reinterpret_cast<const double2 *>(shm + kStages64 * kStage + 2 * kUBytes64);
-  unsigned long long *bar =
-      reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * kUBytes64 + kDXBytes64);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * kUBytes64);
   const bool aligned = (smem_u32(shm) & 127u) == 0;
   if (!aligned && threadIdx.x == 0) atomicExch(D.err, 2);
   if (threadIdx.x == 0 && aligned) {
 #pragma unroll
-    for (int q = 0; q <= kStages64; q++) mbar_init(smem_u32(&bar[q]));  // the ring, then the d^/x^ buffer
+    for (int q = 0; q < kStages64; q++) mbar_init(smem_u32(&bar[q]));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     fence_async_smem();
   }
-  unsigned phase = 0;  // bit q: parity of the next wait on stage q (bit kStages64: d^/x^)
+  unsigned phase = 0;  // bit q: parity of the next wait on stage q
   const long long per_sys = D.tp.count(), total = aligned ? per_sys * D.nsys : 0;
 
   for (;;) {
@@ -1525,28 +1649,17 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   const bool live = i < nx && j < ny;
   const long long N = D.L.N, plane = (long long)D.L.nxp * ny;
   const long long ndc = i + (long long)D.L.nxp * j;
-  const int cur = S->cur;
-  const long long sb = (long long)sys * 4 * N;
+  const int cur = S->cur, pslot = S->pslot;
   double2 *__restrict__ Qw = wvec64(D, cur ^ 1, sys, 0);
   double2 *__restrict__ Vw = wvec64(D, cur ^ 1, sys, 1);
-  double2 *__restrict__ Pw = wvec64(D, cur ^ 1, sys, 2);
-  double2 *__restrict__ dd = D.dd64 + sb;
-  double2 *__restrict__ xx = D.xx64 + sb;
-  const double *__restrict__ sig = D.sig64;
-  const double *__restrict__ eps = D.epsr64;
+  double2 *__restrict__ Pw = pvec64(D, (pslot + 1) % (D.ring64 + 1), sys);
+  const double *__restrict__ sig = D.sig64 + sys * D.mnode;
+  const double *__restrict__ eps = D.epsr64 ? D.epsr64 + sys * D.mnode : nullptr;
   const double ca = S->vscale;
   const double2 cb = rmul(-S->vscale, S->beta);
   const double2 cc = cneg(S->k1);
-  const bool pend = TIMING || S->pending != 0;
-  const double xmix = TIMING ? (double)D.tmix : 1.0;
-  double2 eta = S->eta_pend;
-  double kap = S->kap_pend;
-  if (TIMING) {
-    eta = xmix != 0.0 ? eta : make_double2(0.0, 0.0);
-    kap = xmix != 0.0 ? kap : 1.0;
-  }
   const double ka = S->ka, kb = S->kb;
-  const int wset = cur * D.nsys + sys;
+  const int wset = cur * D.nsys + sys, pset = pslot * D.nsys + sys;
 
   // thread 0: the q^ v^ p^ plane m+1 into stage st (x in 8-byte units: even)
   auto issue = [&](int st, int m) {
@@ -1554,19 +1667,11 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
     fence_async_smem();
     mbar_expect(bb, kStage);
     tma_load5(smem_u32(shm + st * kStage), &M.w64, 2 * (i0 - 2), j0 - 1, m + 1, 0, wset, bb);
+    tma_load5(smem_u32(shm + st * kStage + 8u * kPN * 16u), &M.p64, 2 * (i0 - 2), j0 - 1, m + 1, 0, pset, bb);
   };
   auto wait = [&](int st) {
     if (!mbar_wait(smem_u32(&bar[st]), (phase >> st) & 1u, kWaitTries) && threadIdx.x == 0) atomicExch(D.err, 1);
     phase ^= 1u << st;
-  };
-  // thread 0: d^ and x^ of plane m1's own tile (x origin 2 i0: even)
-  auto issue_dx = [&](int m1) {
-    const unsigned bb = smem_u32(&bar[kStages64]);
-    unsigned char *base = shm + kStages64 * kStage + 2 * kUBytes64;
-    fence_async_smem();
-    mbar_expect(bb, kDXBytes64);
-    tma_load5(smem_u32(base), &M.dd64, 2 * i0, j0, m1, 0, sys, bb);
-    tma_load5(smem_u32(base + kDXBytes64 / 2), &M.xx64, 2 * i0, j0, m1, 0, sys, bb);
   };
   auto combine = [&](double2 q, double2 v, double2 p, double2 &vo) {
     vo = dcfma(cb, v, rmul(ca, q));
@@ -1595,23 +1700,6 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
       }
     }
   };
-  // lagged update of the own node of plane m1 (p^_{n-1} from stage st; d^, x^
-  // with plain loads)
-  auto dx_step = [&](int st, int m1) {
-    if (m1 < k1 && pend) wait(kStages64);
-    if (live && m1 < k1 && pend) {
-      const double2 *R = reinterpret_cast<const double2 *>(shm + st * kStage);
-      const long long nd = ndc + m1 * plane;
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        const long long t = c * N + nd;
-        const double2 d0 = DX[c * kPThreads + threadIdx.x], x0 = DX[(4 + c) * kPThreads + threadIdx.x];
-        const double2 dn = dcfma(eta, R[(8 + c) * kPN + eo], rmul(kap, d0));
-        dd[t] = dn;
-        xx[t] = daxpy(xmix, dn, x0);
-      }
-    }
-  };
   auto halo = [&](int st, double2 *Us) {
     const double2 *R = reinterpret_cast<const double2 *>(shm + st * kStage);
     double2 vt;
@@ -1635,12 +1723,11 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   if (threadIdx.x == 0) {
     issue(0, k0 - 1);
     issue(1, k0);
-    if (pend) issue_dx(k0);
   }
 #pragma unroll
   for (int c = 0; c < 4; c++) um[c] = make_double2(0.0, 0.0);
   if (live && k0 > 0) {
-    const double2 *Qr = wvec64(D, cur, sys, 0), *Vr = wvec64(D, cur, sys, 1), *Pr = wvec64(D, cur, sys, 2);
+    const double2 *Qr = wvec64(D, cur, sys, 0), *Vr = wvec64(D, cur, sys, 1), *Pr = pvec64(D, pslot, sys);
     const long long nd = ndc + (k0 - 1) * plane;
     double2 vt;
 #pragma unroll
@@ -1648,14 +1735,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   }
   wait(0);
   own_step(0, k0, Ub, uc, vc);
-  dx_step(0, k0);
   halo(0, Ub);
   const long long nd0 = ndc + k0 * plane;
   double s2m = sgl(2, nd0 - plane, live && k0 > 0);  // sigma-bar of Az at k0-1
   double e2m = epl(2, nd0 - plane, live && k0 > 0);
   __syncthreads();
   if (threadIdx.x == 0 && k0 + 1 <= k1 - 1) issue(0, k0 + 1);
-  if (threadIdx.x == 0 && pend && k0 + 1 < k1) issue_dx(k0 + 1);
 
   double acc[kParts];
 #pragma unroll
@@ -1766,11 +1851,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
       s2m = sz;
       e2m = ez;
     }
-    dx_step(st, m + 1);
     if (m + 1 < k1) halo(st, Un);
-    __syncthreads();  // everyone is done with stage st, u plane m and the d^/x^ buffer
+    __syncthreads();  // everyone is done with stage st and u plane m
     if (threadIdx.x == 0 && m + 2 <= k1 - 1) issue(st, m + 2);
-    if (threadIdx.x == 0 && pend && m + 2 < k1) issue_dx(m + 2);
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       um[c] = uc[c];
@@ -1789,10 +1872,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   if (arrive<kParts, kPThreads>(blk, part, cnt, (unsigned)tile, nt)) {
     Vals<kParts> tot = final_reduce<kParts, kPThreads>(part, cnt, nt);
     if (threadIdx.x == 0) {
-      if (TIMING)
+      if (TIMING) {
         S->cur ^= 1;
-      else
-        pass_scalars(S, tot.v);
+        S->pslot = (S->pslot + 1) % (D.ring64 + 1);
+      } else {
+        pass_scalars(S, tot.v, D.ring64);
+      }
     }
   }
   }  // work items

@@ -255,10 +255,18 @@ def run_reference(args):
 # ------------------------------------------------------------ GPU arm
 def pass_bytes(nsys, n):
     """Algorithmic bytes of one fused complex64 QMR pass over a batch: per
-    unknown and system read q^, v^, p^, d^, x^ and write q^, v^, p^, d^, x^
-    (10 x 8 B; the Jacobi diagonal is formed on chip), plus the shared FP32
-    sigma-bar once (4 B)."""
-    return nsys * n * 80 + n * 4
+    unknown and system read q^, v^, p^ and write q^, v^, p^ (6 x 8 B; the
+    Jacobi diagonal is formed on chip), plus the shared FP32 sigma-bar once
+    (4 B).  The solution update runs outside the pass, once per R passes
+    (update_bytes)."""
+    return nsys * n * 48 + n * 4
+
+
+def update_bytes(nsys, n, ring):
+    """Algorithmic bytes of one flush of the pending solution updates
+    (k_sw_dxupd): per unknown and system read R p^ slots and d^ (complex64)
+    and x (complex128), write d^ and x"""
+    return nsys * n * ((ring + 2) * 8 + 32)
 
 
 def timed(stream, dev, fn, steps, barrier, world):
@@ -435,13 +443,13 @@ def main():
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("sw_pass_" + args.workload)
-    roofline = {"bound": "hbm", "kernel": "k_sw_pass (fused complex64 QMR iteration: p^ update, "
-                "q^ = D^-1 K p^, lagged d^/x^ update, 12 inner products)",
+    roofline = {"bound": "hbm", "kernel": "k_sw_pass (fused complex64 QMR iteration: v^, p^ update, "
+                "q^ = D^-1 K p^, 12 inner products)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst)",
                 "traffic": traffic, "alg_bytes_per_launch": alg, "launch_us": t_apply * 1e6,
                 "systems_per_launch": len(mine),
-                "units": "80 B per unknown and system + 4 B sigma-bar per unknown"}
+                "units": "48 B per unknown and system + 4 B sigma-bar per unknown"}
 
     # ---- comparisons on the same GPU (rank 0's share at N > 1)
     if not args.no_plain:  # every rank takes the same collective steps
@@ -473,8 +481,9 @@ def main():
     if not args.no_field_err and mine:
         idx = sorted({0, len(mine) // 2, len(mine) - 1})
         extra["field_err"] = field_error(s, m, my_om, my_sos, rec, Ea, Ha, idx)
-    # effective bandwidth of the pass over a whole sweep (all kernels' time)
-    extra["sweep_effective_GBps"] = (sum(it_in) * 80.0 * n) / (ms / args.steps * 1e-3) / 1e9
+    # effective bandwidth of the inner iterations over a whole sweep (all
+    # kernels' time): 48 B per pass and unknown, plus the updates at R = 4
+    extra["sweep_effective_GBps"] = (sum(it_in) * (48.0 + 64.0 / 4) * n) / (ms / args.steps * 1e-3) / 1e9
 
     line = {
         "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,

@@ -194,10 +194,20 @@ int aphid_gpu_inprod_dev(aphid_ctx *ctx, const void *d_k2, const void *d_in,
  * (src/aphid.f90:379-449), real(4) cell arrays (nx-1,ny-1,nz-1).  The
  * area/volume-weighted averages of gen_k2_*grid are formed once on the device
  * in FP64; every system's k^2 follows from them and its omega.  'D'
- * (Cole-Cole) is not linear in omega and is rejected here: use
- * aphid_gpu_gen_k2 + aphid_gpu_qmr per frequency. */
+ * (Cole-Cole) has four cell arrays: aphid_gpu_set_model_cole_cole. */
 int aphid_gpu_set_model(aphid_ctx *ctx, char csig_flag, const float *sig_re,
                         const float *eps_rel);
+
+/* Cole-Cole cell model (read_mesh csig_flag 'D', src/aphid.f90:410-435):
+ * sigma-hat = sigma (1 - eta / (1 + (i omega tau)^c)), real(4) cell arrays
+ * sig_re, eta (chargeability), tau (time constant) and cee (frequency
+ * exponent).  sigma-hat is not linear in omega, so each sweep forms one
+ * averaged model per system on the device (gen_k2_*grid's averages of the
+ * complex sigma-hat at that system's omega): about 80 bytes per unknown and
+ * system beyond the linear models. */
+int aphid_gpu_set_model_cole_cole(aphid_ctx *ctx, const float *sig_re,
+                                  const float *eta, const float *tau,
+                                  const float *cee);
 
 typedef struct {
   int precision;      /* APHID_PREC_FP64, _MIXED, _FUSED64 or _AUTO */
