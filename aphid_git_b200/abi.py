@@ -39,6 +39,13 @@ class Source(C.Structure):
                 ("dip_ijk", C.c_void_p)]
 
 
+class GroupJob(C.Structure):
+    """aphid_group_job: one context's part of a group sweep"""
+    _fields_ = [("ctx", C.c_void_p), ("nsys", C.c_int), ("omega", C.c_void_p),
+                ("source_of_system", C.c_void_p), ("nsrc", C.c_int), ("srcs", C.c_void_p),
+                ("x0", C.c_void_p), ("x_out", C.c_void_p), ("info", C.c_void_p)]
+
+
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("stream", C.c_void_p), ("graph_iters", C.c_int),
                 ("verbose", C.c_int), ("plane_kz", C.c_int)]
@@ -96,6 +103,7 @@ def load():
                                   C.POINTER(SweepOpts), P, P]
     L.aphid_gpu_sweep_sources.argtypes = [P, C.c_int, P, P, C.c_int, P, P, C.POINTER(SweepOpts), P, P]
     L.aphid_gpu_sweep_receivers.argtypes = [P, C.c_int, P, P, P]
+    L.aphid_gpu_sweep_group.argtypes = [C.c_int, P, C.POINTER(SweepOpts)]
     L.aphid_gpu_sweep_fetch.argtypes = [P, C.c_int, P]
     L.aphid_gpu_sweep_time_apply.argtypes = [P, C.c_int]
     L.aphid_gpu_sweep_apply.argtypes = [P, _Z, _Z]
@@ -425,3 +433,44 @@ class Solver:
         self._check(self.lib.aphid_gpu_fields(self._h, float(omega), *self._blocks(sol), *bp,
                                               *ep), "gen_fields")
         return B, E
+
+
+def sweep_group(jobs, precision="auto", target=1e-8, max_it=20000, inner_tol=0.0, max_outer=0,
+                stall_window=0, fetch=True):
+    """Sweeps of several meshes as one batched solve (aphid_gpu_sweep_group).
+
+    jobs: list of (solver, omegas, sources, source_of_system) -- each solver
+    a Solver bound to its own mesh and model, on the same device.  With
+    precision "mixed" or "auto" and models of one kind, the complex64 passes
+    of all meshes share one persistent launch per QMR iteration.  Returns a
+    list of (X, infos) per job, as Solver.sweep returns them."""
+    if not jobs:
+        return []
+    if precision not in PRECISIONS:
+        raise AphidError("precision must be one of %s" % ", ".join(PRECISIONS))
+    o = SweepOpts(PRECISIONS[precision], float(target), int(max_it), float(inner_tol), int(max_outer),
+                  int(stall_window))
+    arr = (GroupJob * len(jobs))()
+    keep, outs = [], []
+    for q, (sv, omegas, sources, sos) in enumerate(jobs):
+        om = np.ascontiguousarray(np.atleast_1d(omegas), dtype=np.float64)
+        nsys = om.size
+        so = np.ascontiguousarray(np.arange(nsys) if sos is None else sos, dtype=np.int32)
+        srcs, k = _sources(sources)
+        X = np.empty((nsys, sv.n), np.complex128) if fetch else None
+        infos = (Info * nsys)()
+        keep += [om, so, srcs, k]
+        outs.append((sv, X, infos, nsys))
+        arr[q] = GroupJob(sv._h.value, nsys, om.ctypes.data, so.ctypes.data, len(sources),
+                          C.cast(srcs, C.c_void_p).value, None, X.ctypes.data if X is not None else None,
+                          C.cast(infos, C.c_void_p).value)
+        sv._last_nsys = 0
+    rc = load().aphid_gpu_sweep_group(len(jobs), arr, C.byref(o))
+    if rc != APHID_OK:
+        msgs = [load().aphid_gpu_last_error(sv._h).decode() for sv, _, _, _ in outs]
+        raise AphidError("sweep_group: %s (%s)" % (ERRORS.get(rc, rc), "; ".join(m for m in msgs if m)))
+    res = []
+    for sv, X, infos, nsys in outs:
+        sv._last_nsys = nsys
+        res.append((X, [i.as_dict() for i in infos]))
+    return res

@@ -87,6 +87,7 @@ struct aphid_ctx {
   int sw_ring64 = 0;         // its R
   double4 *sw_ax64 = nullptr; // FP64 axis tables of the complex128 pass
   int *sw_work = nullptr;    // [2] work counter of the persistent pass, then [order]
+  int *group_work = nullptr; // [2] work counter of group launches led by this context
   int num_sms = 148;         // multiprocessors of the device
   PassMaps maps{};           // TMA tensor maps of the pass
   int *sw_err = nullptr;     // set by a kernel whose bounded wait gave up
@@ -167,6 +168,8 @@ void release_work(aphid_ctx *ctx) {
   ctx->sw_ax64 = nullptr;
   cudaFree(ctx->sw_work);
   ctx->sw_work = nullptr;
+  cudaFree(ctx->group_work);
+  ctx->group_work = nullptr;
   cudaFree(ctx->sw_sys);
   cudaFree(ctx->sw_part);
   cudaFree(ctx->sw_cnt);
@@ -1599,6 +1602,339 @@ int sweep_apply_t(aphid_ctx *ctx, const aphid_z *x, aphid_z *y) {
   return APHID_OK;
 }
 
+// ---------------------------------------------------------------- sweep
+// The phases of a batched sweep: prepare (checks, buffers, model, tuning,
+// right-hand sides, initial state), run (graph rounds; run_batched for one
+// context, run_group for several), finish (escalated systems, info records,
+// solutions to the host).
+struct SweepPrep {
+  int nsys = 0;
+  bool mixed = false, fused = false, batched = false, has_x0 = false;
+  SweepDev D{};
+  std::vector<SweepSys> hs;
+  long long *d_idx = nullptr;
+  double *d_val = nullptr;
+  long long nlaunch = 0;
+  std::vector<aphid_info> out;
+  void release() {
+    cudaFree(d_idx);
+    cudaFree(d_val);
+    d_idx = nullptr;
+    d_val = nullptr;
+  }
+};
+
+int sweep_prepare(aphid_ctx *ctx, int nsys, const double *omega, const int *source_of_system, int nsrc,
+                  const aphid_source *srcs, const aphid_z *x0, const aphid_sweep_opts *opts, SweepPrep &P) {
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->has_model) return fail(ctx, APHID_ERR_STATE, "aphid_gpu_set_model has not been called");
+  if (nsys < 1 || nsrc < 1 || !omega || !source_of_system || !srcs || !opts)
+    return fail(ctx, APHID_ERR_BADARG, "sweep: bad counts or null arrays");
+  for (int q = 0; q < nsrc; q++) {
+    const aphid_source &S = srcs[q];
+    if (S.oper_mode != 2 && S.oper_mode != 3 && S.oper_mode != 5)
+      return fail(ctx, APHID_ERR_BADARG, "sweep: a source's oper_mode must be 2, 3 or 5");
+    if (S.oper_mode == 5 && S.ndip < 0) return fail(ctx, APHID_ERR_BADARG, "negative dipole count");
+    if (S.oper_mode == 5 && S.ndip > 0 && (!S.dip_dir || !S.dip_ijk))
+      return fail(ctx, APHID_ERR_BADARG, "null dipole arrays");
+  }
+  for (int s = 0; s < nsys; s++) {
+    if (source_of_system[s] < 0 || source_of_system[s] >= nsrc)
+      return fail(ctx, APHID_ERR_BADARG, "source index out of range");
+    if (!std::isfinite(omega[s])) return fail(ctx, APHID_ERR_BADARG, "non-finite omega");
+  }
+  const int prec = opts->precision;
+  const bool mixed = prec == APHID_PREC_MIXED || prec == APHID_PREC_AUTO;
+  const bool fused = prec == APHID_PREC_FUSED64;
+  if (!mixed && !fused && prec != APHID_PREC_FP64) return fail(ctx, APHID_ERR_BADARG, "unknown precision");
+  if (!(opts->target >= 0.0) || opts->max_it < 0) return fail(ctx, APHID_ERR_BADARG, "bad target or max_it");
+  if ((mixed || fused) && 4 * ctx->nl.N >= (1LL << 31))
+    return fail(ctx, APHID_ERR_BADARG, "batched sweep: more than 2^31 node-layout values per system");
+  // from here on the buffers are rebuilt for this call: until it succeeds,
+  // the post-sweep hooks (time_apply, apply, fetch) must refuse the old state
+  ctx->sw_last = 0;
+  if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
+  if (fused && (rc = sweep_alloc64(ctx, nsys))) return rc;
+  if ((rc = ensure_work(ctx))) return rc;
+  if (ctx->csig == 'D') {
+    // the model follows the frequencies: one averaged sigma-hat per system
+    if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
+    ctx->sw_gexec = nullptr;
+    if ((rc = build_cole_cole(ctx, nsys, omega))) return rc;
+  }
+  if (mixed || fused) {
+    if (ctx->plane_kz > 0) {
+      if (ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) && (rc = plane_tiles(ctx, ctx->plane_kz)))
+        return rc;
+    } else if ((rc = tune_kz(ctx, nsys, fused))) {
+      return rc;
+    }
+  }
+
+  // sources -> sparse right-hand sides
+  std::vector<std::map<long long, double>> src;
+  source_entries(ctx, nsrc, srcs, src);
+  std::vector<long long> eidx;
+  std::vector<double> eval;
+  for (int s = 0; s < nsys; s++)
+    for (const auto &kv : src[source_of_system[s]]) {
+      eidx.push_back((long long)s * ctx->n + kv.first);
+      eval.push_back(kv.second);
+    }
+  P.D = sweep_dev(ctx, nsys);
+  const size_t vec = (size_t)nsys * ctx->n;
+  CK(cudaMemsetAsync(P.D.b, 0, vec * sizeof(double2), ctx->stream));
+  if (!eidx.empty()) {
+    CK(cudaMalloc(&P.d_idx, eidx.size() * sizeof(long long)));
+    CK(cudaMalloc(&P.d_val, eval.size() * sizeof(double)));
+    CK(cudaMemcpyAsync(P.d_idx, eidx.data(), eidx.size() * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(P.d_val, eval.data(), eval.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    k_sw_scatter<<<(unsigned)((eidx.size() + 255) / 256), 256, 0, ctx->stream>>>((long long)eidx.size(), P.d_idx,
+                                                                                 P.d_val, P.D.b);
+  }
+  if (x0)
+    CK(cudaMemcpyAsync(P.D.x64, x0, vec * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  else
+    CK(cudaMemsetAsync(P.D.x64, 0, vec * sizeof(double2), ctx->stream));
+  P.nsys = nsys;
+  P.mixed = mixed;
+  P.fused = fused;
+  P.batched = mixed || fused;
+  P.has_x0 = x0 != nullptr;
+  P.hs.resize(nsys);
+  for (int s = 0; s < nsys; s++)
+    P.hs[s] = sweep_sys_init(omega[s], opts, fused, prec == APHID_PREC_AUTO, opts->max_it, ctx->csig);
+  P.out.assign(nsys, aphid_info{});
+  return APHID_OK;
+}
+
+// the reference's own algorithm, one system at a time, on resident data
+int run_plain(aphid_ctx *ctx, SweepPrep &P, const aphid_sweep_opts *opts) {
+  int rc;
+  double2 *k2 = wv(ctx, W_K2), *dg = wv(ctx, W_INV);
+  for (int s = 0; s < P.nsys; s++) {
+    const long long mo = ctx->csig == 'D' ? (long long)s * ctx->n : 0;
+    k_sw_k2vec<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_sig + mo,
+                                                               ctx->d_epsr ? ctx->d_epsr + mo : nullptr, P.hs[s].ka,
+                                                               P.hs[s].kb, k2);
+    k_gen_diag<<<node_grid(ctx), 128, 0, ctx->stream>>>(ctx->g, k2, dg);
+    CK(cudaMemcpyAsync(wv(ctx, W_B), P.D.b + (size_t)s * ctx->n, ctx->n * sizeof(double2), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(wv(ctx, W_X), P.D.x64 + (size_t)s * ctx->n, ctx->n * sizeof(double2),
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+    ctx->loaded = true;
+    ctx->inv_ready = false;
+    aphid_info I{};
+    if ((rc = qmr_run(ctx, opts->target, opts->max_it, P.has_x0, nullptr, 0, &I))) return rc;
+    CK(cudaMemcpyAsync(P.D.x64 + (size_t)s * ctx->n, wv(ctx, W_X), ctx->n * sizeof(double2),
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+    P.nlaunch += 2 + I.kernel_launches;
+    I.inner64_iters = I.iters;
+    P.out[s] = I;
+  }
+  ctx->loaded = false;
+  return APHID_OK;
+}
+
+// after run_batched / run_group (P.hs read back) or run_plain: the escalated
+// systems (AUTO), the info records and the solutions to the host.  With
+// own_events the sweep's time is ctx's ev0 .. now; otherwise info->seconds is
+// filled by the caller.
+int sweep_finish(aphid_ctx *ctx, SweepPrep &P, const double *omega, const aphid_sweep_opts *opts, aphid_z *x_out,
+                 aphid_info *info, bool own_events) {
+  int rc;
+  if (P.batched) {
+    for (int s = 0; s < P.nsys; s++) P.out[s] = sweep_info(P.hs[s], P.fused);
+    std::vector<int> esc;
+    for (int s = 0; s < P.nsys; s++)
+      if (P.hs[s].status == kStEscalated) esc.push_back(s);
+    if (!esc.empty() && (rc = finish_escalated(ctx, omega, opts, esc, P.out, P.nlaunch))) return rc;
+  }
+  float ms = 0.f;
+  if (own_events) {
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  } else {
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  for (int s = 0; s < P.nsys; s++) {
+    if (own_events) P.out[s].seconds = ms * 1e-3;
+    P.out[s].kernel_launches = P.nlaunch;
+    if (info) info[s] = P.out[s];
+  }
+  ctx->sw_last = P.nsys;
+  ctx->sw_last_fused = P.fused;
+  ctx->sw_omega.assign(omega, omega + P.nsys);
+  if (x_out) {
+    CK(cudaMemcpyAsync(x_out, P.D.x64, (size_t)P.nsys * ctx->n * sizeof(double2), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return APHID_OK;
+}
+
+// Several contexts' complex64 sweeps as one: per graph round every context's
+// flush and outer step, then graph_iters launches of k_sw_pass_group, whose
+// persistent blocks take the work items of all meshes from one counter, with
+// every context's flush after each R of them (R the smallest ring of the
+// group), and every context's monitor.  Runs on the first job's stream.
+int run_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opts) {
+  aphid_ctx *c0 = jobs[0].ctx;
+  int rc;
+  std::vector<SweepPrep> P(njob);
+  for (int a = 0; a < njob; a++) {
+    const aphid_group_job &J = jobs[a];
+    if ((rc = sweep_prepare(J.ctx, J.nsys, J.omega, J.source_of_system, J.nsrc, J.srcs, J.x0, opts, P[a]))) {
+      for (auto &q : P) q.release();
+      return rc;
+    }
+  }
+  for (int a = 0; a < njob; a++) {
+    const cudaError_t e = cudaStreamSynchronize(jobs[a].ctx->stream);
+    if (e != cudaSuccess) {
+      for (auto &q : P) q.release();
+      return cuda_fail(jobs[a].ctx, e, "group: preparing a sweep");
+    }
+  }
+  aphid_ctx *ctx = c0;  // CK reports on the first context
+  const cudaStream_t st = c0->stream;
+  const bool eps = c0->d_epsr32 != nullptr;
+  // items of every mesh, the larger meshes first
+  std::vector<int> ord(njob);
+  for (int a = 0; a < njob; a++) ord[a] = a;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+    return P[a].D.tp.count() * P[a].D.nsys > P[b].D.tp.count() * P[b].D.nsys;
+  });
+  PassGroup G{};
+  G.n = njob;
+  int ring = kMaxRing;
+  for (int q = 0; q < njob; q++) {
+    const int a = ord[q];
+    G.D[q] = P[a].D;
+    G.M[q] = jobs[a].ctx->maps;
+    G.first[q + 1] = G.first[q] + P[a].D.tp.count() * P[a].D.nsys;
+    ring = std::min(ring, P[a].D.ring);
+  }
+  while (c0->graph_iters % ring) ring /= 2;
+  if (!c0->group_work) {
+    CK(cudaMalloc(&c0->group_work, 2 * sizeof(int)));
+  }
+  CK(cudaMemsetAsync(c0->group_work, 0, 2 * sizeof(int), st));
+  G.work = c0->group_work;
+  int per_sm = eps ? PassShm<true>::blocks : PassShm<false>::blocks;
+  const size_t shm = eps ? PassShm<true>::bytes : PassShm<false>::bytes;
+  if (eps)
+    CK(cudaFuncSetAttribute(k_sw_pass_group<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+  else
+    CK(cudaFuncSetAttribute(k_sw_pass_group<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+  const unsigned grid = (unsigned)std::min<long long>(G.first[njob], (long long)per_sm * c0->num_sms);
+  for (int a = 0; a < njob; a++) {
+    aphid_ctx *c = jobs[a].ctx;
+    if ((rc = pass_attrs(c))) return rc;
+    CK(cudaMemcpyAsync(c->sw_sys, P[a].hs.data(), P[a].nsys * sizeof(SweepSys), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(c->sw_ndone, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(c->sw_err, 0, sizeof(int), st));
+    k_sw_bnorm<<<(unsigned)(P[a].D.bps * P[a].nsys), kStreamThreads, 0, st>>>(P[a].D);
+  }
+  CK(cudaGetLastError());
+  // the round as a graph
+  cudaGraph_t graph;
+  cudaGraphExec_t gexec = nullptr;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  auto flush = [&]() {
+    for (int a = 0; a < njob; a++) {
+      const SweepDev &D = P[a].D;
+      k_sw_dxupd<float2, false><<<(unsigned)(D.bps * D.nsys), kStreamThreads, 0, st>>>(D);
+    }
+  };
+  flush();
+  for (int a = 0; a < njob; a++) {
+    const SweepDev &D = P[a].D;
+    k_sw_resid<float2><<<(unsigned)(D.t.count() * D.nsys), kOpThreads, 0, st>>>(D);
+  }
+  for (int it = 0; it < c0->graph_iters; it++) {
+    if (eps)
+      k_sw_pass_group<true, false><<<grid, kPThreads, shm, st>>>(G);
+    else
+      k_sw_pass_group<false, false><<<grid, kPThreads, shm, st>>>(G);
+    if ((it + 1) % ring == 0) flush();
+  }
+  for (int a = 0; a < njob; a++) {
+    const SweepDev &D = P[a].D;
+    k_sw_check<float2><<<(unsigned)(D.t.count() * D.nsys), kOpThreads, 0, st>>>(D);
+  }
+  cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (e != cudaSuccess) return cuda_fail(c0, e, "group: graph capture");
+  e = cudaGraphInstantiate(&gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(c0, e, "group: cudaGraphInstantiate");
+  const long long per_round =
+      (long long)njob * (3 + c0->graph_iters / ring) + c0->graph_iters;
+  long long max_rounds = 0, nlaunch = njob;
+  for (int a = 0; a < njob; a++)
+    max_rounds = std::max<long long>(max_rounds, (long long)std::max(1, opts->max_it) / c0->graph_iters +
+                                                     2LL * (P[a].hs[0].max_outer + 2));
+  CK(cudaEventRecord(c0->ev0, st));
+  rc = APHID_OK;
+  for (long long round = 0;; round++) {
+    bool all = true;
+    for (int a = 0; a < njob && !rc; a++) {
+      aphid_ctx *c = jobs[a].ctx;
+      e = cudaMemcpyAsync(c->h_ndone, c->sw_ndone, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) rc = cuda_fail(c0, e, "group: progress");
+    }
+    if (!rc && (e = cudaStreamSynchronize(st)) != cudaSuccess) rc = cuda_fail(c0, e, "group: round");
+    if (rc) break;
+    for (int a = 0; a < njob; a++) all = all && *jobs[a].ctx->h_ndone >= P[a].nsys;
+    if (all) break;
+    if (round > max_rounds) {
+      rc = fail(c0, APHID_ERR_STATE, "group sweep did not terminate");
+      break;
+    }
+    if ((e = cudaGraphLaunch(gexec, st)) != cudaSuccess) {
+      rc = cuda_fail(c0, e, "group: graph launch");
+      break;
+    }
+    nlaunch += per_round;
+  }
+  cudaGraphExecDestroy(gexec);
+  float ms = 0.f;
+  if (!rc) {
+    CK(cudaEventRecord(c0->ev1, st));
+    CK(cudaEventSynchronize(c0->ev1));
+    CK(cudaEventElapsedTime(&ms, c0->ev0, c0->ev1));
+  }
+  for (int a = 0; a < njob && !rc; a++) {
+    aphid_ctx *c = jobs[a].ctx;
+    int kerr = 0;
+    if ((e = cudaMemcpy(P[a].hs.data(), c->sw_sys, P[a].nsys * sizeof(SweepSys), cudaMemcpyDeviceToHost)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(&kerr, c->sw_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+      rc = cuda_fail(c, e, "group: results");
+      break;
+    }
+    if (kerr) {
+      rc = fail(c, APHID_ERR_CUDA, "group sweep: a tensor-copy wait in the operator pass timed out");
+      break;
+    }
+    P[a].nlaunch = nlaunch;
+    // the escalated systems (AUTO) of each context finish on its own stream
+    if ((rc = sweep_finish(c, P[a], jobs[a].omega, opts, jobs[a].x_out, jobs[a].info, false))) break;
+    if (jobs[a].info)
+      for (int s = 0; s < P[a].nsys; s++) jobs[a].info[s].seconds = ms * 1e-3;
+  }
+  for (auto &q : P) q.release();
+  // the single-context graphs hold stale launch geometry for these buffers
+  for (int a = 0; a < njob; a++) {
+    aphid_ctx *c = jobs[a].ctx;
+    if (c->sw_gexec) cudaGraphExecDestroy(c->sw_gexec);
+    c->sw_gexec = nullptr;
+  }
+  return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1684,141 +2020,45 @@ int aphid_gpu_sweep(aphid_ctx *ctx, int nsys, const double *omega, const int *so
 int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega, const int *source_of_system, int nsrc,
                             const aphid_source *srcs, const aphid_z *x0, const aphid_sweep_opts *opts,
                             aphid_z *x_out, aphid_info *info) {
-  int rc = check_ready(ctx);
+  SweepPrep P;
+  int rc = sweep_prepare(ctx, nsys, omega, source_of_system, nsrc, srcs, x0, opts, P);
   if (rc) return rc;
-  if (!ctx->has_model) return fail(ctx, APHID_ERR_STATE, "aphid_gpu_set_model has not been called");
-  if (nsys < 1 || nsrc < 1 || !omega || !source_of_system || !srcs || !opts || !info)
-    return fail(ctx, APHID_ERR_BADARG, "sweep: bad counts or null arrays");
-  for (int q = 0; q < nsrc; q++) {
-    const aphid_source &S = srcs[q];
-    if (S.oper_mode != 2 && S.oper_mode != 3 && S.oper_mode != 5)
-      return fail(ctx, APHID_ERR_BADARG, "sweep: a source's oper_mode must be 2, 3 or 5");
-    if (S.oper_mode == 5 && S.ndip < 0) return fail(ctx, APHID_ERR_BADARG, "negative dipole count");
-    if (S.oper_mode == 5 && S.ndip > 0 && (!S.dip_dir || !S.dip_ijk))
-      return fail(ctx, APHID_ERR_BADARG, "null dipole arrays");
-  }
-  for (int s = 0; s < nsys; s++) {
-    if (source_of_system[s] < 0 || source_of_system[s] >= nsrc)
-      return fail(ctx, APHID_ERR_BADARG, "source index out of range");
-    if (!std::isfinite(omega[s])) return fail(ctx, APHID_ERR_BADARG, "non-finite omega");
-  }
-  const int prec = opts->precision;
-  const bool mixed = prec == APHID_PREC_MIXED || prec == APHID_PREC_AUTO;
-  const bool fused = prec == APHID_PREC_FUSED64;
-  if (!mixed && !fused && prec != APHID_PREC_FP64) return fail(ctx, APHID_ERR_BADARG, "unknown precision");
-  if (!(opts->target >= 0.0) || opts->max_it < 0) return fail(ctx, APHID_ERR_BADARG, "bad target or max_it");
-  if ((mixed || fused) && 4 * ctx->nl.N >= (1LL << 31))
-    return fail(ctx, APHID_ERR_BADARG, "batched sweep: more than 2^31 node-layout values per system");
-  // from here on the buffers are rebuilt for this call: until it succeeds,
-  // the post-sweep hooks (time_apply, apply, fetch) must refuse the old state
-  ctx->sw_last = 0;
-  if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
-  if (fused && (rc = sweep_alloc64(ctx, nsys))) return rc;
-  if ((rc = ensure_work(ctx))) return rc;
-  if (ctx->csig == 'D') {
-    // the model follows the frequencies: one averaged sigma-hat per system
-    if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
-    ctx->sw_gexec = nullptr;
-    if ((rc = build_cole_cole(ctx, nsys, omega))) return rc;
-  }
-  if (mixed || fused) {
-    if (ctx->plane_kz > 0) {
-      if (ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) && (rc = plane_tiles(ctx, ctx->plane_kz)))
-        return rc;
-    } else if ((rc = tune_kz(ctx, nsys, fused))) {
-      return rc;
-    }
-  }
-
-  // sources -> sparse right-hand sides
-  std::vector<std::map<long long, double>> src;
-  source_entries(ctx, nsrc, srcs, src);
-  std::vector<long long> eidx;
-  std::vector<double> eval;
-  for (int s = 0; s < nsys; s++)
-    for (const auto &kv : src[source_of_system[s]]) {
-      eidx.push_back((long long)s * ctx->n + kv.first);
-      eval.push_back(kv.second);
-    }
-  SweepDev D = sweep_dev(ctx, nsys);
-  const size_t vec = (size_t)nsys * ctx->n;
-  double2 *b = D.b, *x64 = D.x64;
-  long long *d_idx = nullptr;
-  double *d_val = nullptr;
-  CK(cudaMemsetAsync(b, 0, vec * sizeof(double2), ctx->stream));
-  if (!eidx.empty()) {
-    CK(cudaMalloc(&d_idx, eidx.size() * sizeof(long long)));
-    CK(cudaMalloc(&d_val, eval.size() * sizeof(double)));
-    CK(cudaMemcpyAsync(d_idx, eidx.data(), eidx.size() * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(d_val, eval.data(), eval.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    k_sw_scatter<<<(unsigned)((eidx.size() + 255) / 256), 256, 0, ctx->stream>>>((long long)eidx.size(), d_idx,
-                                                                                 d_val, b);
-  }
-  if (x0)
-    CK(cudaMemcpyAsync(x64, x0, vec * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
-  else
-    CK(cudaMemsetAsync(x64, 0, vec * sizeof(double2), ctx->stream));
-
-  std::vector<SweepSys> hs(nsys);
-  for (int s = 0; s < nsys; s++)
-    hs[s] = sweep_sys_init(omega[s], opts, fused, prec == APHID_PREC_AUTO, opts->max_it, ctx->csig);
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  long long nlaunch = 0;
-  std::vector<aphid_info> out(nsys);
+  if (P.batched)
+    rc = run_batched(ctx, P.D, P.fused, P.hs, opts->max_it, P.nlaunch);
+  else
+    rc = run_plain(ctx, P, opts);
+  if (!rc) rc = sweep_finish(ctx, P, omega, opts, x_out, info, true);
+  P.release();
+  return rc;
+}
 
-  if (mixed || fused) {
-    if ((rc = run_batched(ctx, D, fused, hs, opts->max_it, nlaunch))) return rc;
-    for (int s = 0; s < nsys; s++) out[s] = sweep_info(hs[s], fused);
-    std::vector<int> esc;
-    for (int s = 0; s < nsys; s++)
-      if (hs[s].status == kStEscalated) esc.push_back(s);
-    if (!esc.empty() && (rc = finish_escalated(ctx, omega, opts, esc, out, nlaunch))) return rc;
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-  } else {
-    // the reference's own algorithm, one system at a time, on resident data
-    double2 *k2 = wv(ctx, W_K2), *dg = wv(ctx, W_INV);
-    for (int s = 0; s < nsys; s++) {
-      const long long mo = ctx->csig == 'D' ? (long long)s * ctx->n : 0;
-      k_sw_k2vec<<<ctx->sblk, kStreamThreads, 0, ctx->stream>>>(ctx->n, ctx->d_sig + mo,
-                                                                 ctx->d_epsr ? ctx->d_epsr + mo : nullptr, hs[s].ka,
-                                                                 hs[s].kb, k2);
-      k_gen_diag<<<node_grid(ctx), 128, 0, ctx->stream>>>(ctx->g, k2, dg);
-      CK(cudaMemcpyAsync(wv(ctx, W_B), b + (size_t)s * ctx->n, ctx->n * sizeof(double2),
-                         cudaMemcpyDeviceToDevice, ctx->stream));
-      CK(cudaMemcpyAsync(wv(ctx, W_X), x64 + (size_t)s * ctx->n, ctx->n * sizeof(double2),
-                         cudaMemcpyDeviceToDevice, ctx->stream));
-      ctx->loaded = true;
-      ctx->inv_ready = false;
-      aphid_info I{};
-      if ((rc = qmr_run(ctx, opts->target, opts->max_it, x0 != nullptr, nullptr, 0, &I))) return rc;
-      CK(cudaMemcpyAsync(x64 + (size_t)s * ctx->n, wv(ctx, W_X), ctx->n * sizeof(double2),
-                         cudaMemcpyDeviceToDevice, ctx->stream));
-      nlaunch += 2 + I.kernel_launches;
-      I.inner64_iters = I.iters;
-      out[s] = I;
+int aphid_gpu_sweep_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opts) {
+  if (njob < 1 || njob > kMaxGroup || !jobs || !opts) return APHID_ERR_BADARG;
+  for (int a = 0; a < njob; a++) {
+    if (!jobs[a].ctx) return APHID_ERR_BADARG;
+    for (int b = 0; b < a; b++)
+      if (jobs[a].ctx == jobs[b].ctx) return fail(jobs[a].ctx, APHID_ERR_BADARG, "group: a context appears twice");
+    if (jobs[a].ctx->device != jobs[0].ctx->device)
+      return fail(jobs[a].ctx, APHID_ERR_BADARG, "group: all contexts must be on one device");
+  }
+  const bool mixed = opts->precision == APHID_PREC_MIXED || opts->precision == APHID_PREC_AUTO;
+  bool same_kind = true;
+  for (int a = 0; a < njob; a++)
+    same_kind = same_kind && jobs[a].ctx->has_model && ((jobs[a].ctx->d_epsr32 != nullptr) ==
+                                                        (jobs[0].ctx->d_epsr32 != nullptr)) &&
+                jobs[a].ctx->csig != 'D' && jobs[0].ctx->csig != 'D';
+  if (!mixed || !same_kind || njob == 1) {
+    // nothing to share in one launch: the jobs one after another
+    for (int a = 0; a < njob; a++) {
+      const aphid_group_job &J = jobs[a];
+      const int rc = aphid_gpu_sweep_sources(J.ctx, J.nsys, J.omega, J.source_of_system, J.nsrc, J.srcs, J.x0, opts,
+                                             J.x_out, J.info);
+      if (rc) return rc;
     }
-    ctx->loaded = false;
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    return APHID_OK;
   }
-  float ms = 0.f;
-  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-  cudaFree(d_idx);
-  cudaFree(d_val);
-  for (int s = 0; s < nsys; s++) {
-    out[s].seconds = ms * 1e-3;
-    out[s].kernel_launches = nlaunch;
-    info[s] = out[s];
-  }
-  ctx->sw_last = nsys;
-  ctx->sw_last_fused = fused;
-  ctx->sw_omega.assign(omega, omega + nsys);
-  if (x_out) {
-    CK(cudaMemcpyAsync(x_out, x64, vec * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-  }
-  return APHID_OK;
+  return run_group(njob, jobs, opts);
 }
 
 int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {

@@ -53,6 +53,16 @@
         integer(c_int) :: reserved(2)
       end type aphid_sweep_opts
 
+      ! a source of aphid_gpu_sweep_sources: oper_mode 2 / 3 (MT sheet
+      ! sources of gen_rhs) or 5 (ndip dipoles, dip_dir "+X".."-Z" and
+      ! 1-based tail nodes dip_ijk; c_null_ptr for MT)
+      type, bind(C) :: aphid_source
+        integer(c_int) :: oper_mode
+        integer(c_int) :: ndip
+        type(c_ptr)    :: dip_dir
+        type(c_ptr)    :: dip_ijk
+      end type aphid_source
+
       interface
         integer(c_int) function aphid_gpu_create(ctx, opts)             &
                        bind(C, name="aphid_gpu_create")
@@ -128,6 +138,45 @@
           type(c_ptr), value :: x0, x_out
           type(aphid_sweep_opts), intent(in) :: opts
           type(aphid_info), intent(out) :: info(*)
+        end function
+
+        ! the same with sources of any kind: the MT farm (aphid_mpi.input
+        ! 'MT') passes srcs = [aphid_source(2, ...), aphid_source(3, ...)]
+        integer(c_int) function aphid_gpu_sweep_sources(ctx, nsys,      &
+                       omega, source_of_system, nsrc, srcs, x0, opts,   &
+                       x_out, info)                                     &
+                       bind(C, name="aphid_gpu_sweep_sources")
+          import :: c_int, c_ptr, c_double, aphid_source,               &
+                    aphid_sweep_opts, aphid_info
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: nsys, nsrc
+          real(c_double), intent(in) :: omega(*)
+          integer(c_int), intent(in) :: source_of_system(*)
+          type(aphid_source), intent(in) :: srcs(*)
+          type(c_ptr), value :: x0, x_out
+          type(aphid_sweep_opts), intent(in) :: opts
+          type(aphid_info), intent(out) :: info(*)
+        end function
+
+        ! Cole-Cole cells (csig_flag 'D'): sig_re, eta, tau, cee
+        integer(c_int) function aphid_gpu_set_model_cole_cole(ctx,      &
+                       sig_re, eta, tau, cee)                           &
+                       bind(C, name="aphid_gpu_set_model_cole_cole")
+          import :: c_int, c_ptr, c_float
+          type(c_ptr), value :: ctx
+          real(c_float), intent(in) :: sig_re(*), eta(*), tau(*), cee(*)
+        end function
+
+        ! E and H at 1-based interior nodes rec_ijk(3, nrec) for every
+        ! system of the last sweep: E, H (3, nrec, nsys)
+        integer(c_int) function aphid_gpu_sweep_receivers(ctx, nrec,    &
+                       rec_ijk, e, h)                                   &
+                       bind(C, name="aphid_gpu_sweep_receivers")
+          import :: c_int, c_ptr, c_double_complex
+          type(c_ptr), value :: ctx
+          integer(c_int), value :: nrec
+          integer(c_int), intent(in) :: rec_ijk(*)
+          complex(c_double_complex), intent(out) :: e(*), h(*)
         end function
       end interface
 

@@ -271,6 +271,32 @@ int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega,
                             const aphid_sweep_opts *opts, aphid_z *x_out,
                             aphid_info *info);
 
+/* Several meshes in one batched solve.  Each job is one context (its own
+ * mesh and model, set with aphid_gpu_set_mesh / aphid_gpu_set_model) with
+ * its own systems, sources, optional x0, optional x_out and info records,
+ * exactly the arguments of aphid_gpu_sweep_sources.  With precision MIXED or
+ * AUTO and models of one kind (R, or C and I), the complex64 QMR passes of
+ * all jobs run as one persistent launch per iteration whose blocks take work
+ * items from every mesh, so systems of uneven mesh sizes share the GPU
+ * without a launch per mesh; escalated systems (AUTO) then finish per
+ * context.  Other precisions, Cole-Cole models, mixed model kinds or a single
+ * job run the jobs one after another.  All contexts must be on one device;
+ * the shared work runs on the first job's stream, and info->seconds is the
+ * group's time.  At most 8 jobs. */
+typedef struct {
+  aphid_ctx *ctx;
+  int nsys;
+  const double *omega;
+  const int *source_of_system;
+  int nsrc;
+  const aphid_source *srcs;
+  const aphid_z *x0;   /* nullable */
+  aphid_z *x_out;      /* nullable */
+  aphid_info *info;    /* nullable */
+} aphid_group_job;
+int aphid_gpu_sweep_group(int njob, const aphid_group_job *jobs,
+                          const aphid_sweep_opts *opts);
+
 /* Receiver gather after a sweep: E and H = B / mu0 at nrec mesh nodes for
  * every system of the last sweep, without moving the solutions to the host.
  * The node values are dump_fields' EM_grid interpolation

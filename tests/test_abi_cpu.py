@@ -114,8 +114,9 @@ def _c_struct_fields(header, name):
         decl = decl.strip()
         if not decl:
             continue
-        names = decl.split(None, 1)[1] if not decl.startswith("long long") else decl.split(None, 2)[2]
-        fields += [n.strip().lstrip("*").split("[")[0] for n in names.split(",")]
+        # "int a, b", "const char *p", "long long n", "int r[2]": the last
+        # word of each comma-separated part is a field name
+        fields += [part.replace("*", " ").split()[-1].split("[")[0] for part in decl.split(",")]
     return fields
 
 
@@ -138,5 +139,5 @@ def test_fortran_binding_types_match_the_c_structs():
         header = f.read()
     with open(os.path.join(root, "aphid_git_b200", "fortran", "aphid_gpu_mod.f90")) as f:
         src = f.read()
-    for name in ("aphid_opts", "aphid_info", "aphid_sweep_opts"):
+    for name in ("aphid_opts", "aphid_info", "aphid_sweep_opts", "aphid_source"):
         assert _fortran_type_fields(src, name) == _c_struct_fields(header, name), name

@@ -147,6 +147,42 @@ def test_sweep_cole_cole_matches_oracle(solver, precision):
         assert relerr(e1, e0) < 1e-6 and relerr(b1, b0) < 1e-6, (s, relerr(e1, e0), relerr(b1, b0))
 
 
+@pytest.mark.parametrize("precision", ["mixed", "auto"])
+def test_sweep_group_of_uneven_meshes(precision):
+    """Two meshes of different sizes, one batched solve (aphid_gpu_sweep_group):
+    the complex64 passes of both share each launch.  Every system converges
+    to the FP64 target, its true residual against the oracle's operator holds
+    it, and the solutions agree with each mesh solved on its own to the
+    tolerance of two converged 1e-8 solves of the same system."""
+    from aphid_git_b200.abi import sweep_group
+    cases = [small_model(seed=31, dims=(22, 19, 21), nair=4), small_model(seed=32, dims=(14, 12, 13))]
+    srcs = [[[("+X", 10, 9, 5)], [("+Y", 9, 9, 5)]], [[("+X", 6, 6, 4)]]]
+    freqs = [[0.05, 3.0, 200.0], [0.5, 40.0]]
+    solvers, jobs = [], []
+    for (xn, yn, zn, sig, _), sr, fr in zip(cases, srcs, freqs):
+        sv = Solver(graph_iters=8)
+        sv.set_nodes(xn, yn, zn)
+        sv.set_model("R", sig)
+        om = [2 * np.pi * f for f in fr for _ in sr]
+        sos = [q for _ in fr for q in range(len(sr))]
+        solvers.append(sv)
+        jobs.append((sv, om, sr, sos))
+    try:
+        res = sweep_group(jobs, precision=precision, target=1e-8)
+        for (sv, om, sr, sos), (X, infos), (xn, yn, zn, sig, _) in zip(jobs, res, cases):
+            g = O.Grid(xn, yn, zn)
+            X1, inf1 = sv.sweep(om, sr, sos, precision=precision, target=1e-8)
+            for s, w in enumerate(om):
+                assert infos[s]["status_name"] == "converged", infos[s]
+                k2 = O.gen_k2(g, model.sigma_hat("R", w, sig.ravel(order="F")), w)
+                b, _ = O.gen_rhs(g, 5, sr[sos[s]])
+                assert np.linalg.norm(b - O.inprod(g, k2, X[s])) / np.linalg.norm(b) < 2e-8
+                assert relerr(X[s], X1[s]) < 1e-5, (s, relerr(X[s], X1[s]))
+    finally:
+        for sv in solvers:
+            sv.close()
+
+
 def test_sweep_halfspace32_mixed(solver):
     m = model.make_model("halfspace32")
     solver.set_nodes(m.xn, m.yn, m.zn)
