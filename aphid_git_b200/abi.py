@@ -154,6 +154,7 @@ def _sources(sources):
 
 
 NOALLOC_MAX_NODES = 1024
+NOALLOC_MAX_SLOTS = 16384
 
 
 def inprod_eps_noalloc(nx, ny, nz, d_spacing, d_k2, d_in, d_out, d_eps, stream=0):

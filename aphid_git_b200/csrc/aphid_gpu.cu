@@ -1385,9 +1385,13 @@ int swap_systems(aphid_ctx *ctx, int p, int q, double2 *tmp) {
 // their current iterates, in as few chunks as device memory allows.  Each
 // chunk is moved to the front slots (the batched kernels address systems
 // 0..k-1), solved, and moved back.
+// keep_whole: when one chunk held every system of the sweep in its own slot
+// order (a FUSED64 sweep that fits), keep the complex128 buffers for the
+// post-sweep hooks instead of releasing them.
 int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts *opts, const std::vector<int> &esc,
-                     std::vector<aphid_info> &out, long long &nlaunch) {
+                     std::vector<aphid_info> &out, long long &nlaunch, bool keep_whole = false) {
   int rc = APHID_OK;
+  bool whole = false;
   // the complex64 buffers are not needed again by this call: give their memory
   // to the complex128 ones (the next mixed sweep re-allocates them)
   if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
@@ -1413,6 +1417,8 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
   const size_t have =
       fr + (ctx->sw_w64 ? (size_t)ctx->sw_nsys64 * (6 + ctx->sw_ring64) * 4 * ctx->nl.N * sizeof(double2) : 0);
   const int cap = (int)std::max<size_t>(1, std::min<size_t>(esc.size(), (have - std::min(have, (size_t)1 << 30)) / per));
+  whole = cap >= (int)esc.size() && (int)esc.size() == ctx->sw_nsys;
+  for (size_t q = 0; q < esc.size() && whole; q++) whole = esc[q] == (int)q;
   for (size_t c0 = 0; c0 < esc.size() && !rc; c0 += cap) {
     const int k = (int)std::min<size_t>(cap, esc.size() - c0);
     if ((rc = sweep_alloc64(ctx, k))) break;
@@ -1457,13 +1463,16 @@ int finish_escalated(aphid_ctx *ctx, const double *omega, const aphid_sweep_opts
   }
   const cudaError_t se = cudaStreamSynchronize(ctx->stream);
   cudaFree(tmp);
+  whole = whole && keep_whole && !rc;
   // the complex128 buffers were sized for this phase only: release them, so
   // that the next mixed sweep has the memory it had
   if (ctx->sw_gexec) cudaGraphExecDestroy(ctx->sw_gexec);
   ctx->sw_gexec = nullptr;
-  cudaFree(ctx->sw_w64);
-  ctx->sw_w64 = nullptr;
-  ctx->sw_nsys64 = 0;
+  if (!whole) {
+    cudaFree(ctx->sw_w64);
+    ctx->sw_w64 = nullptr;
+    ctx->sw_nsys64 = 0;
+  }
   if (!rc && se != cudaSuccess) rc = cuda_fail(ctx, se, "sweep (escalated systems)");
   return rc;
 }
@@ -1654,8 +1663,9 @@ int sweep_prepare(aphid_ctx *ctx, int nsys, const double *omega, const int *sour
   // from here on the buffers are rebuilt for this call: until it succeeds,
   // the post-sweep hooks (time_apply, apply, fetch) must refuse the old state
   ctx->sw_last = 0;
+  // FUSED64 allocates its complex128 buffers in run_fused, in as many chunks
+  // of systems as memory holds
   if ((rc = sweep_alloc(ctx, nsys, mixed))) return rc;
-  if (fused && (rc = sweep_alloc64(ctx, nsys))) return rc;
   if ((rc = ensure_work(ctx))) return rc;
   if (ctx->csig == 'D') {
     // the model follows the frequencies: one averaged sigma-hat per system
@@ -1667,7 +1677,7 @@ int sweep_prepare(aphid_ctx *ctx, int nsys, const double *omega, const int *sour
     if (ctx->plane_kz > 0) {
       if (ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) && (rc = plane_tiles(ctx, ctx->plane_kz)))
         return rc;
-    } else if ((rc = tune_kz(ctx, nsys, fused))) {
+    } else if (mixed && (rc = tune_kz(ctx, nsys, false))) {  // FUSED64 tunes per chunk in run_fused
       return rc;
     }
   }
@@ -1700,13 +1710,27 @@ int sweep_prepare(aphid_ctx *ctx, int nsys, const double *omega, const int *sour
   P.nsys = nsys;
   P.mixed = mixed;
   P.fused = fused;
-  P.batched = mixed || fused;
+  P.batched = mixed;
   P.has_x0 = x0 != nullptr;
   P.hs.resize(nsys);
   for (int s = 0; s < nsys; s++)
     P.hs[s] = sweep_sys_init(omega[s], opts, fused, prec == APHID_PREC_AUTO, opts->max_it, ctx->csig);
   P.out.assign(nsys, aphid_info{});
   return APHID_OK;
+}
+
+// FUSED64: the batched complex128 pass over every system from its initial
+// iterate, through the chunked path AUTO uses for its escalated systems
+// (one chunk when the systems fit; the buffers are then kept for the
+// post-sweep hooks)
+int run_fused(aphid_ctx *ctx, SweepPrep &P, const double *omega, const aphid_sweep_opts *opts) {
+  std::vector<int> all(P.nsys);
+  for (int s = 0; s < P.nsys; s++) all[s] = s;
+  // the chunks start from the current iterates x (zero or x0) and count
+  // from zero
+  P.out.assign(P.nsys, aphid_info{});
+  for (int s = 0; s < P.nsys; s++) P.out[s].rhs_norm = 0.0;
+  return finish_escalated(ctx, omega, opts, all, P.out, P.nlaunch, true);
 }
 
 // the reference's own algorithm, one system at a time, on resident data
@@ -2026,6 +2050,8 @@ int aphid_gpu_sweep_sources(aphid_ctx *ctx, int nsys, const double *omega, const
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (P.batched)
     rc = run_batched(ctx, P.D, P.fused, P.hs, opts->max_it, P.nlaunch);
+  else if (P.fused)
+    rc = run_fused(ctx, P, omega, opts);
   else
     rc = run_plain(ctx, P, opts);
   if (!rc) rc = sweep_finish(ctx, P, omega, opts, x_out, info, true);

@@ -755,15 +755,25 @@ static __global__ void __launch_bounds__(kStreamThreads) k_sw_dxupd(SweepDev D) 
     for (int c = 0; c < 4; c++) {
       if (!exists(g, c, i, j, k)) continue;
       const long long t = c * D.L.N + nd;
-      T d = dd[t];
-      double2 dx = make_double2(0.0, 0.0);
-      for (int q = 0; q < np; q++) {
-        d = dx_link(s_eta[q], __ldg(s_p[q] + t), s_kap[q], d);
-        dx = cadd(dx, to_d(d));
-      }
-      dd[t] = d;
       const long long rt = ref_of(g, c, i, j, k);
-      x64[rt] = make_double2(fma(mix, dx.x, x64[rt].x), fma(mix, dx.y, x64[rt].y));
+      // every load of this unknown first (the ring slots, d^, x), then the
+      // recurrence: the loads are in flight together instead of one memory
+      // latency per pending update
+      T pj[kMaxRing];
+#pragma unroll
+      for (int q = 0; q < kMaxRing; q++)
+        if (q < np) pj[q] = __ldg(s_p[q] + t);
+      T d = dd[t];
+      const double2 x0 = x64[rt];
+      double2 dx = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < kMaxRing; q++)
+        if (q < np) {
+          d = dx_link(s_eta[q], pj[q], s_kap[q], d);
+          dx = cadd(dx, to_d(d));
+        }
+      dd[t] = d;
+      x64[rt] = make_double2(fma(mix, dx.x, x0.x), fma(mix, dx.y, x0.y));
     }
   }
   // the last block of this system empties its pending list

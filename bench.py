@@ -293,16 +293,26 @@ def timed(stream, dev, fn, steps, barrier, world):
 def field_error(s, m, om, sos, rec, Ea, Ha, idx):
     """relative error of E and H at the receivers of systems idx (from a
     finished sweep: Ea, Ha) against complex128 solves of the reference's
-    recurrence to 1e-12"""
-    s.sweep([om[q] for q in idx], m.sources, [sos[q] for q in idx], precision="fp64",
-            target=1e-12, max_it=4 * MAX_IT, fetch=False)
+    recurrence to 1e-12, beside the error of that recurrence itself stopped at
+    the same 1e-8 target (a 1e-8 residual does not bound every field error:
+    at 1e5 Hz in seawater the fields 2 km from the source are rounding noise
+    of the source region's).  bound = max(1e-6, 2 x the reference's own)."""
+    sub = ([om[q] for q in idx], m.sources, [sos[q] for q in idx])
+    s.sweep(*sub, precision="fp64", target=1e-12, max_it=4 * MAX_IT, fetch=False)
     Er, Hr = s.sweep_receivers(rec)
+    s.sweep(*sub, precision="fp64", target=TARGET, max_it=4 * MAX_IT, fetch=False)
+    E8, H8 = s.sweep_receivers(rec)
     err = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     e = [err(Ea[q], Er[r]) for r, q in enumerate(idx)]
     h = [err(Ha[q], Hr[r]) for r, q in enumerate(idx)]
-    return {"E": max(e), "H": max(h), "per_system": {"freq_hz": [om[q] / (2 * np.pi) for q in idx],
-                                                      "E": e, "H": h},
+    e8 = [err(E8[r], Er[r]) for r in range(len(idx))]
+    h8 = [err(H8[r], Hr[r]) for r in range(len(idx))]
+    ok = all(a <= max(1e-6, 2 * b) for a, b in zip(e + h, e8 + h8))
+    return {"E": max(e), "H": max(h), "within_bound": ok,
+            "per_system": {"freq_hz": [om[q] / (2 * np.pi) for q in idx], "E": e, "H": h,
+                           "E_reference_at_1e-8": e8, "H_reference_at_1e-8": h8},
             "reference": "complex128 Jacobi-QMR (reference recurrence) to 1e-12",
+            "bound": "max(1e-6, 2 x the reference recurrence's own error at 1e-8)",
             "receivers": int(len(rec))}
 
 
@@ -395,7 +405,15 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    ms, infs = timed(stream, dev, sweep, args.steps, barrier, world)
+    def farm_sweep():
+        # N > 1: the farm deals the systems by predicted cost, each rank solves
+        # its share in one batched sweep, and E, H at the receivers are
+        # gathered to rank 0 (the solutions stay on the ranks' devices)
+        _, inf = farm.sweep(s, om, m.sources, sos, rank=rank, world=world, dist=dist, receivers=rec,
+                            precision=args.precision, target=TARGET, max_it=MAX_IT, inner_tol=args.inner_tol)
+        return [inf[q] for q in mine] if inf is not None else []
+
+    ms, infs = timed(stream, dev, farm_sweep if world > 1 else sweep, args.steps, barrier, world)
     clk = clocks.stop()
     last = infs[-1]
     launches = int(sum(i[0]["kernel_launches"] for i in infs if i))
@@ -472,15 +490,22 @@ def main():
             with open(ITERS_FILE, "w") as f:
                 json.dump(d, f, indent=1)
     if not args.no_fused64:
-        ms_f, inf_f = timed(stream, dev, lambda: sweep("fused64"), 1, barrier, world)
-        fi = inf_f[-1] or [{"inner_iters": 0, "status_name": "none"}]
-        extra["fused64_sweep"] = {"time_s": ms_f * 1e-3, "iters": [i["inner_iters"] for i in fi],
-                                  "status": sorted({i["status_name"] for i in fi}),
-                                  "note": "batched complex128 pass (k_sw_pass64) for every system"}
-        extra["speedup_vs_fused64_sweep"] = ms_f / (ms / args.steps)
+        try:
+            ms_f, inf_f = timed(stream, dev, lambda: sweep("fused64"), 1, barrier, world)
+            fi = inf_f[-1] or [{"inner_iters": 0, "status_name": "none"}]
+            extra["fused64_sweep"] = {"time_s": ms_f * 1e-3, "iters": [i["inner_iters"] for i in fi],
+                                      "status": sorted({i["status_name"] for i in fi}),
+                                      "note": "batched complex128 pass (k_sw_pass64) for every system, in "
+                                              "as many chunks as device memory holds"}
+            extra["speedup_vs_fused64_sweep"] = ms_f / (ms / args.steps)
+        except Exception as e:  # a comparison leg: report, keep the line
+            extra["fused64_sweep"] = {"error": str(e)}
     if not args.no_field_err and mine:
-        idx = sorted({0, len(mine) // 2, len(mine) - 1})
-        extra["field_err"] = field_error(s, m, my_om, my_sos, rec, Ea, Ha, idx)
+        try:
+            idx = sorted({0, len(mine) // 2, len(mine) - 1})
+            extra["field_err"] = field_error(s, m, my_om, my_sos, rec, Ea, Ha, idx)
+        except Exception as e:
+            extra["field_err"] = {"error": str(e)}
     # effective bandwidth of the inner iterations over a whole sweep (all
     # kernels' time): 48 B per pass and unknown, plus the updates at R = 4
     extra["sweep_effective_GBps"] = (sum(it_in) * (48.0 + 64.0 / 4) * n) / (ms / args.steps * 1e-3) / 1e9
@@ -506,9 +531,12 @@ def main():
             iters, src = recorded_iters(args.workload)
             src = "recorded: %s" % src
         if iters:
-            spi, done, cores = cpu_sample(m, args.cpu_sample_iters)
-            line["cpu_baseline"] = cpu_baseline_obj(spi, done, cores, iters, src, nsys)
-            line["cpu_baseline"]["extrapolated"] = True
+            try:
+                spi, done, cores = cpu_sample(m, args.cpu_sample_iters)
+                line["cpu_baseline"] = cpu_baseline_obj(spi, done, cores, iters, src, nsys)
+                line["cpu_baseline"]["extrapolated"] = True
+            except Exception as e:
+                line["cpu_baseline"] = {"error": str(e)}
     s.close()
     if rank == 0:
         print(json.dumps(line))
