@@ -108,6 +108,7 @@ def load():
     L.aphid_gpu_sweep_time_apply.argtypes = [P, C.c_int]
     L.aphid_gpu_sweep_apply.argtypes = [P, _Z, _Z]
     L.aphid_gpu_sweep_plane_kz.argtypes = [P]
+    L.aphid_gpu_sweep_pass_config.argtypes = [P]
     _lib = L
     return L
 
@@ -416,6 +417,11 @@ class Solver:
         """z-planes per work item of the complex64 pass in use (the
         autotuner's choice unless plane_kz was fixed); 0 before a mixed sweep."""
         return int(self.lib.aphid_gpu_sweep_plane_kz(self._h))
+
+    def sweep_pass_config(self):
+        """pipeline configuration of the complex64 pass in use (0: two load
+        stages, two blocks per SM for model R; 1: three stages, one block)"""
+        return int(self.lib.aphid_gpu_sweep_pass_config(self._h))
 
     def sweep_fetch(self, sys):
         x = np.empty(self.n, np.complex128)

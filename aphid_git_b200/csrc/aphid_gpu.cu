@@ -85,6 +85,7 @@ struct aphid_ctx {
   double2 *sw_w64 = nullptr; // the complex128 pass's q^ v^ (2 sets), p^ ring, d^: the sw_f32 layout
   int sw_nsys64 = 0;         // systems sw_w64 holds
   int sw_ring64 = 0;         // its R
+  int pass_cfg = 0;          // pipeline configuration of the complex64 pass (PassShm CFG), tuned
   double4 *sw_ax64 = nullptr; // FP64 axis tables of the complex128 pass
   int *sw_work = nullptr;    // [2] work counter of the persistent pass, then [order]
   int *group_work = nullptr; // [2] work counter of group launches led by this context
@@ -1053,15 +1054,27 @@ static __global__ void k_sw_scatter(long long cnt, const long long *__restrict__
   if (t < cnt) b[idx[t]] = make_double2(val[t], 0.0);
 }
 
-size_t pass_shm(const SweepDev &D) { return D.epsr32 ? PassShm<true>::bytes : PassShm<false>::bytes; }
+size_t pass_shm(const SweepDev &D, int cfg) {
+  return D.epsr32 ? (cfg ? PassShm<true, 1>::bytes : PassShm<true, 0>::bytes)
+                  : (cfg ? PassShm<false, 1>::bytes : PassShm<false, 0>::bytes);
+}
+int pass_blocks(const SweepDev &D, int cfg) {
+  return D.epsr32 ? (cfg ? PassShm<true, 1>::blocks : PassShm<true, 0>::blocks)
+                  : (cfg ? PassShm<false, 1>::blocks : PassShm<false, 0>::blocks);
+}
 
 // opt in to the dynamic shared memory of the pass (once per context)
 int pass_attrs(aphid_ctx *ctx) {
-  const int r = (int)PassShm<false>::bytes, e = (int)PassShm<true>::bytes;
-  CK(cudaFuncSetAttribute(k_sw_pass<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, r));
-  CK(cudaFuncSetAttribute(k_sw_pass<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, r));
-  CK(cudaFuncSetAttribute(k_sw_pass<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
-  CK(cudaFuncSetAttribute(k_sw_pass<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
+  const int r0 = (int)PassShm<false, 0>::bytes, e0 = (int)PassShm<true, 0>::bytes;
+  const int r1 = (int)PassShm<false, 1>::bytes, e1 = (int)PassShm<true, 1>::bytes;
+  CK(cudaFuncSetAttribute(k_sw_pass<false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, r0));
+  CK(cudaFuncSetAttribute(k_sw_pass<false, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, r0));
+  CK(cudaFuncSetAttribute(k_sw_pass<true, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, e0));
+  CK(cudaFuncSetAttribute(k_sw_pass<true, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, e0));
+  CK(cudaFuncSetAttribute(k_sw_pass<false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, r1));
+  CK(cudaFuncSetAttribute(k_sw_pass<false, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, r1));
+  CK(cudaFuncSetAttribute(k_sw_pass<true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, e1));
+  CK(cudaFuncSetAttribute(k_sw_pass<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, e1));
   const int f = (int)kPass64Shm;
   CK(cudaFuncSetAttribute(k_sw_pass64<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
   CK(cudaFuncSetAttribute(k_sw_pass64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
@@ -1070,23 +1083,32 @@ int pass_attrs(aphid_ctx *ctx) {
   return APHID_OK;
 }
 
-// persistent: PassShm<EPS>::blocks resident blocks per SM
-void launch_pass(aphid_ctx *ctx, const SweepDev &D, bool timing) {
-  const long long items = D.tp.count() * D.nsys;
-  const int per_sm = D.epsr32 ? PassShm<true>::blocks : PassShm<false>::blocks;
-  const unsigned sp = (unsigned)std::min<long long>(items, (long long)per_sm * ctx->num_sms);
-  const size_t shm = pass_shm(D);
+template <int CFG>
+void launch_pass_cfg(aphid_ctx *ctx, const SweepDev &D, bool timing, unsigned sp, size_t shm) {
   if (D.epsr32) {
     if (timing)
-      k_sw_pass<true, true><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+      k_sw_pass<true, true, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
     else
-      k_sw_pass<true, false><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+      k_sw_pass<true, false, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
   } else {
     if (timing)
-      k_sw_pass<false, true><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+      k_sw_pass<false, true, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
     else
-      k_sw_pass<false, false><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
+      k_sw_pass<false, false, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
   }
+}
+
+// persistent: PassShm<EPS, CFG>::blocks resident blocks per SM, in the
+// pipeline configuration the tuner chose (ctx->pass_cfg)
+void launch_pass(aphid_ctx *ctx, const SweepDev &D, bool timing) {
+  const long long items = D.tp.count() * D.nsys;
+  const int cfg = ctx->pass_cfg;
+  const unsigned sp = (unsigned)std::min<long long>(items, (long long)pass_blocks(D, cfg) * ctx->num_sms);
+  const size_t shm = pass_shm(D, cfg);
+  if (cfg)
+    launch_pass_cfg<1>(ctx, D, timing, sp, shm);
+  else
+    launch_pass_cfg<0>(ctx, D, timing, sp, shm);
 }
 
 // the complex128 pass, persistent like launch_pass
@@ -1160,43 +1182,48 @@ int sweep_graph(aphid_ctx *ctx, const SweepDev &D, bool fused64) {
 // and a hash of its name, so ranks on different GPU models keep their own
 // choices.
 typedef std::array<int, 7> TuneKey;  // nx, ny, nz, nsys, eps-bar present + 2 x complex128 pass, SMs, name hash
+// A tuned choice: z-slab depth kz and pipeline configuration cfg of the pass
+struct Tuned {
+  int kz = 0, cfg = 0;
+};
+
 
 std::mutex &tune_mutex() {
   static std::mutex m;
   return m;
 }
-std::map<TuneKey, int> &tune_cache() {
-  static std::map<TuneKey, int> m;
+std::map<TuneKey, Tuned> &tune_cache() {
+  static std::map<TuneKey, Tuned> m;
   return m;
 }
 
-int tune_file_lookup(const TuneKey &k) {
+Tuned tune_file_lookup(const TuneKey &k) {
+  Tuned found;
   const char *path = std::getenv("APHID_TUNE_CACHE");
-  if (!path || !*path) return 0;
+  if (!path || !*path) return found;
   FILE *f = std::fopen(path, "r");
-  if (!f) return 0;
+  if (!f) return found;
   char line[256];
-  int found = 0;
   while (std::fgets(line, sizeof line, f)) {
-    int v[8];
+    int v[9];
     char tail;
-    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %c", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7],
-                    &tail) != 8)
+    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %c", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7],
+                    &v[8], &tail) != 9)
       continue;  // torn, foreign or old-format record
-    bool same = v[7] >= kMinKz;
+    bool same = v[7] >= kMinKz && (v[8] == 0 || v[8] == 1);
     for (int q = 0; q < 7; q++) same = same && v[q] == k[q];
-    if (same) found = v[7];
+    if (same) found = Tuned{v[7], v[8]};
   }
   std::fclose(f);
   return found;
 }
 
-void tune_file_store(const TuneKey &k, int kz) {
+void tune_file_store(const TuneKey &k, Tuned t) {
   const char *path = std::getenv("APHID_TUNE_CACHE");
   if (!path || !*path) return;
   char line[160];
-  const int len = std::snprintf(line, sizeof line, "%d %d %d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4], k[5],
-                                k[6], kz);
+  const int len = std::snprintf(line, sizeof line, "%d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4], k[5],
+                                k[6], t.kz, t.cfg);
   if (len <= 0 || len >= (int)sizeof line) return;
   const int fd = ::open(path, O_WRONLY | O_APPEND | O_CREAT, 0644);
   if (fd < 0) return;
@@ -1219,66 +1246,74 @@ void device_identity(const aphid_ctx *ctx, int &sms, int &name_hash) {
   name_hash = (int)(h & 0x7fffffff);
 }
 
+// The complex64 pass is timed for every (kz, cfg): the z-slab depths and the
+// two pipeline configurations of PassShm (two stages with two blocks per SM
+// for model R, or three stages in one); the complex128 pass for kz alone.
 int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
   int sms, name_hash;
   device_identity(ctx, sms, name_hash);
   const TuneKey key = {ctx->nx, ctx->ny, ctx->nz, nsys, (ctx->d_epsr32 ? 1 : 0) + (fused ? 2 : 0), sms, name_hash};
-  int kz = 0;
+  Tuned best;
   {
     std::lock_guard<std::mutex> lock(tune_mutex());
     auto it = tune_cache().find(key);
-    if (it != tune_cache().end()) kz = it->second;
+    if (it != tune_cache().end()) best = it->second;
   }
-  if (!kz) kz = tune_file_lookup(key);
+  if (!best.kz) best = tune_file_lookup(key);
   int rc;
-  if (!kz) {
+  if (!best.kz) {
     int rc0 = pass_attrs(ctx);
     if (rc0) return rc0;
     CK(cudaMemsetAsync(ctx->sw_sys, 0, (size_t)nsys * sizeof(SweepSys), ctx->stream));
     CK(cudaMemsetAsync(ctx->sw_err, 0, sizeof(int), ctx->stream));
     float best_ms = 0.f;
     const int cand[] = {4, 6, 8, 12, 16, 24, 32};
-    int last_tk = -1;
-    for (int c : cand) {
-      if (c > ctx->nz) break;
-      const int tk = (ctx->nz + c - 1) / c;
-      if (tk == last_tk) continue;  // same slabs as the previous candidate
-      last_tk = tk;
-      if ((rc = plane_tiles(ctx, c))) return rc;
-      SweepDev D = sweep_dev(ctx, nsys);
-      D.tmix = 0.f;
-      auto pass = [&]() {
-        if (fused)
-          launch_pass64(ctx, D, true);
-        else
-          launch_pass(ctx, D, true);
-      };
-      for (int r = 0; r < 2; r++) pass();
-      CK(cudaEventRecord(ctx->ev0, ctx->stream));
-      for (int r = 0; r < 5; r++) pass();
-      CK(cudaEventRecord(ctx->ev1, ctx->stream));
-      CK(cudaEventSynchronize(ctx->ev1));
-      CK(cudaGetLastError());
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-      if (!kz || ms < best_ms) {
-        kz = c;
-        best_ms = ms;
+    for (int cfg = 0; cfg < (fused ? 1 : 2); cfg++) {
+      int last_tk = -1;
+      for (int c : cand) {
+        if (c > ctx->nz) break;
+        const int tk = (ctx->nz + c - 1) / c;
+        if (tk == last_tk) continue;  // same slabs as the previous candidate
+        last_tk = tk;
+        if ((rc = plane_tiles(ctx, c))) return rc;
+        ctx->pass_cfg = cfg;
+        SweepDev D = sweep_dev(ctx, nsys);
+        D.tmix = 0.f;
+        auto pass = [&]() {
+          if (fused)
+            launch_pass64(ctx, D, true);
+          else
+            launch_pass(ctx, D, true);
+        };
+        for (int r = 0; r < 2; r++) pass();
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        for (int r = 0; r < 5; r++) pass();
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        CK(cudaEventSynchronize(ctx->ev1));
+        CK(cudaGetLastError());
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        if (!best.kz || ms < best_ms) {
+          best = Tuned{c, cfg};
+          best_ms = ms;
+        }
+        if (ctx->verbose)
+          std::fprintf(stderr, "aphid_gpu: tune kz=%d cfg=%d %.3f ms/pass%s\n", c, cfg, ms / 5, fused ? " (c128)" : "");
       }
-      if (ctx->verbose) std::fprintf(stderr, "aphid_gpu: tune kz=%d %.3f ms/pass%s\n", c, ms / 5, fused ? " (c128)" : "");
     }
     int kerr = 0;
     CK(cudaMemcpy(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (kerr) return fail(ctx, APHID_ERR_CUDA, "tuner: a tensor-copy wait in the pass timed out");
-    if (!kz) kz = default_kz(ctx, nsys);
-    tune_file_store(key, kz);
+    if (!best.kz) best = Tuned{default_kz(ctx, nsys), 0};
+    tune_file_store(key, best);
   }
   {
     std::lock_guard<std::mutex> lock(tune_mutex());
-    tune_cache()[key] = kz;
+    tune_cache()[key] = best;
   }
-  if (ctx->ptiles.kz != kz || !ctx->sw_work) {
-    if ((rc = plane_tiles(ctx, kz))) return rc;
+  if (!fused) ctx->pass_cfg = best.cfg;
+  if (ctx->ptiles.kz != best.kz || !ctx->sw_work) {
+    if ((rc = plane_tiles(ctx, best.kz))) return rc;
   }
   return APHID_OK;
 }
@@ -1847,12 +1882,16 @@ int run_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opt
   }
   CK(cudaMemsetAsync(c0->group_work, 0, 2 * sizeof(int), st));
   G.work = c0->group_work;
-  int per_sm = eps ? PassShm<true>::blocks : PassShm<false>::blocks;
-  const size_t shm = eps ? PassShm<true>::bytes : PassShm<false>::bytes;
+  // the group runs in the pipeline configuration of the first context
+  const int cfg = c0->pass_cfg;
+  const int per_sm = pass_blocks(P[0].D, cfg);
+  const size_t shm = pass_shm(P[0].D, cfg);
   if (eps)
-    CK(cudaFuncSetAttribute(k_sw_pass_group<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    CK(cudaFuncSetAttribute(cfg ? k_sw_pass_group<true, false, 1> : k_sw_pass_group<true, false, 0>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
   else
-    CK(cudaFuncSetAttribute(k_sw_pass_group<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    CK(cudaFuncSetAttribute(cfg ? k_sw_pass_group<false, false, 1> : k_sw_pass_group<false, false, 0>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
   const unsigned grid = (unsigned)std::min<long long>(G.first[njob], (long long)per_sm * c0->num_sms);
   for (int a = 0; a < njob; a++) {
     aphid_ctx *c = jobs[a].ctx;
@@ -1879,10 +1918,17 @@ int run_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opt
     k_sw_resid<float2><<<(unsigned)(D.t.count() * D.nsys), kOpThreads, 0, st>>>(D);
   }
   for (int it = 0; it < c0->graph_iters; it++) {
-    if (eps)
-      k_sw_pass_group<true, false><<<grid, kPThreads, shm, st>>>(G);
-    else
-      k_sw_pass_group<false, false><<<grid, kPThreads, shm, st>>>(G);
+    if (eps) {
+      if (cfg)
+        k_sw_pass_group<true, false, 1><<<grid, kPThreads, shm, st>>>(G);
+      else
+        k_sw_pass_group<true, false, 0><<<grid, kPThreads, shm, st>>>(G);
+    } else {
+      if (cfg)
+        k_sw_pass_group<false, false, 1><<<grid, kPThreads, shm, st>>>(G);
+      else
+        k_sw_pass_group<false, false, 0><<<grid, kPThreads, shm, st>>>(G);
+    }
     if ((it + 1) % ring == 0) flush();
   }
   for (int a = 0; a < njob; a++) {
@@ -2109,6 +2155,11 @@ int aphid_gpu_sweep_time_apply(aphid_ctx *ctx, int reps) {
 int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx) {
   if (!ctx) return APHID_ERR_BADARG;
   return ctx->sw_work ? ctx->ptiles.kz : 0;
+}
+
+int aphid_gpu_sweep_pass_config(aphid_ctx *ctx) {
+  if (!ctx) return APHID_ERR_BADARG;
+  return ctx->pass_cfg;
 }
 
 int aphid_gpu_sweep_apply(aphid_ctx *ctx, const aphid_z *x, aphid_z *y) {

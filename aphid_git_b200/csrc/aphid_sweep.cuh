@@ -986,16 +986,18 @@ constexpr unsigned kVecPlane = kPN * 8u;         // one component of one vector,
 constexpr unsigned kRawBytes = 12u * kVecPlane;  // q^, v^, p^ with halo, four components each
 constexpr unsigned kSigBytes = 4u * kKN * 4u;    // sigma-bar with halo, four components
 constexpr unsigned kUBytes = 4u * kVecPlane;     // u of one plane
-// Shared memory and occupancy of the pass.  Model R: two load stages
-// (41.5 KB each) and two blocks per SM (16 warps, at most 128 registers per
-// thread); models C, I and D stage eps-bar too and run three stages in one
-// block per SM.  Each stage holds q^ v^ (8 components) and p^ (4) of plane
-// m+1 with halo and sigma-bar [eps-bar] of plane m; then two u planes and the
-// mbarriers.
-template <bool EPS>
+// Shared memory and occupancy of the pass, in two pipeline configurations
+// that the autotuner chooses between per mesh and batch: CFG 0, two load
+// stages, with two resident blocks per SM for model R (16 warps, at most 128
+// registers per thread); CFG 1, three load stages in one block per SM.
+// Models C, I and D stage eps-bar too and fit one block per SM in both.  Each
+// stage holds q^ v^ (8 components) and p^ (4) of plane m+1 with halo and
+// sigma-bar [eps-bar] of plane m (41.5 KB, 48.4 KB with eps-bar); then two u
+// planes and the mbarriers.
+template <bool EPS, int CFG>
 struct PassShm {
-  static constexpr int stages = EPS ? 3 : 2;
-  static constexpr int blocks = EPS ? 1 : 2;  // resident blocks per SM
+  static constexpr int stages = CFG == 0 ? 2 : 3;
+  static constexpr int blocks = (EPS || CFG == 1) ? 1 : 2;  // resident blocks per SM
   static constexpr unsigned sig = kRawBytes;
   static constexpr unsigned stage = kRawBytes + (EPS ? 2u : 1u) * kSigBytes;
   static constexpr size_t bytes = stages * (size_t)stage + 2 * (size_t)kUBytes + 128;
@@ -1179,10 +1181,10 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T, int ring
 // One work item (a tile's z-slab of one system) of the complex64 pass, on
 // the mesh and buffers of D with the tensor maps M.  shm: the pass's dynamic
 // shared memory; bar, phase: its stage mbarriers and their wait parities.
-template <bool EPS, bool TIMING>
+template <bool EPS, bool TIMING, int CFG>
 __device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, long long item,
                                           unsigned char *shm, unsigned long long *bar, unsigned &phase) {
-  using SH = PassShm<EPS>;
+  using SH = PassShm<EPS, CFG>;
   constexpr int kStages = SH::stages;
   constexpr unsigned kStage = SH::stage;
   float2 *Ub = reinterpret_cast<float2 *>(shm + kStages * kStage);  // [2][4][kPN]
@@ -1476,10 +1478,10 @@ __device__ __forceinline__ void pass_block_done(int *work) {
   }
 }
 
-template <bool EPS, bool TIMING>
-__global__ void __launch_bounds__(kPThreads, PassShm<EPS>::blocks) k_sw_pass(SweepDev D,
-                                                                            const __grid_constant__ PassMaps M) {
-  using SH = PassShm<EPS>;
+template <bool EPS, bool TIMING, int CFG>
+__global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG>::blocks) k_sw_pass(SweepDev D,
+                                                                                 const __grid_constant__ PassMaps M) {
+  using SH = PassShm<EPS, CFG>;
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * kUBytes);
@@ -1492,7 +1494,7 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS>::blocks) k_sw_pass(Swe
     __syncthreads();
     const long long item = s_item;
     if (item >= total) break;
-    pass_item<EPS, TIMING>(D, M, item, shm, bar, phase);
+    pass_item<EPS, TIMING, CFG>(D, M, item, shm, bar, phase);
   }
   pass_block_done(D.work);
 }
@@ -1511,9 +1513,9 @@ struct PassGroup {
   PassMaps M[kMaxGroup];
 };
 
-template <bool EPS, bool TIMING>
-__global__ void __launch_bounds__(kPThreads, PassShm<EPS>::blocks) k_sw_pass_group(const __grid_constant__ PassGroup G) {
-  using SH = PassShm<EPS>;
+template <bool EPS, bool TIMING, int CFG>
+__global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG>::blocks) k_sw_pass_group(const __grid_constant__ PassGroup G) {
+  using SH = PassShm<EPS, CFG>;
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * kUBytes);
@@ -1528,7 +1530,7 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS>::blocks) k_sw_pass_gro
     if (item >= total) break;
     int m = 0;
     while (m + 1 < G.n && item >= G.first[m + 1]) m++;
-    pass_item<EPS, TIMING>(G.D[m], G.M[m], item - G.first[m], shm, bar, phase);
+    pass_item<EPS, TIMING, CFG>(G.D[m], G.M[m], item - G.first[m], shm, bar, phase);
   }
   pass_block_done(G.work);
 }

@@ -314,6 +314,12 @@ int aphid_gpu_sweep_receivers(aphid_ctx *ctx, int nrec, const int *rec_ijk,
  * sweep. */
 int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx);
 
+/* Pipeline configuration of the complex64 pass in use: 0 = two load stages
+ * (two resident blocks per SM for model R), 1 = three load stages in one
+ * block per SM; chosen with the slab depth by the autotuner (0 when
+ * aphid_opts.plane_kz fixes the depth). */
+int aphid_gpu_sweep_pass_config(aphid_ctx *ctx);
+
 /* Copy system `sys` of the last sweep into x (one [x|y|z|p] vector). */
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);
 

@@ -344,13 +344,14 @@ def test_autotuner_picks_and_caches_the_slab_depth(tmp_path, monkeypatch):
         s.set_model("R", sig)
         X1, i1 = s.sweep(w, src, [0, 0])
         kz = s.sweep_plane_kz()
-        assert kz in (4, 6, 8, 12, 16, 24, 32) and kz <= len(zn)
+        cfg = s.sweep_pass_config()
+        assert kz in (4, 6, 8, 12, 16, 24, 32) and kz <= len(zn) and cfg in (0, 1)
         X2, _ = s.sweep(w, src, [0, 0])
         assert s.sweep_plane_kz() == kz          # cached, not retuned
         assert np.array_equal(X1, X2)            # same depth, same bits
     rec = cache.read_text().split()
     sms, name_hash = _device_identity()
-    assert rec[-8:] == [str(v) for v in (18, 17, 26, 2, 0, sms, name_hash, kz)]
+    assert rec[-9:] == [str(v) for v in (18, 17, 26, 2, 0, sms, name_hash, kz, cfg)]
     with Solver(graph_iters=8, plane_kz=8) as s:
         s.set_nodes(xn, yn, zn)
         s.set_model("R", sig)
@@ -377,7 +378,7 @@ def test_tune_cache_file_is_per_device_and_skips_torn_records(tmp_path, monkeypa
     is skipped, and this device's record is taken without retuning."""
     sms, name_hash = _device_identity()
     cache = tmp_path / "tune.txt"
-    cache.write_text("15 14 13 1 0 %d %d 16\n15 14 13 1 0 %d\n15 14 13 1 0 %d %d 6\n"
+    cache.write_text("15 14 13 1 0 %d %d 16 0\n15 14 13 1 0 %d\n15 14 13 1 0 %d %d 6 1\n"
                      % (sms + 4, name_hash, sms, sms, name_hash))
     monkeypatch.setenv("APHID_TUNE_CACHE", str(cache))
     xn, yn, zn, sig, _ = small_model(seed=12, dims=(15, 14, 13))
@@ -386,7 +387,7 @@ def test_tune_cache_file_is_per_device_and_skips_torn_records(tmp_path, monkeypa
         s.set_model("R", sig)
         _, inf = s.sweep([2 * np.pi], [[("+X", 7, 7, 4)]], [0])
         assert inf[0]["status_name"] == "converged"
-        assert s.sweep_plane_kz() == 6
+        assert s.sweep_plane_kz() == 6 and s.sweep_pass_config() == 1
     assert len(cache.read_text().splitlines()) == 3  # taken from the file: nothing appended
 
 
