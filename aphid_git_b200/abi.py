@@ -109,6 +109,7 @@ def load():
     L.aphid_gpu_sweep_apply.argtypes = [P, _Z, _Z]
     L.aphid_gpu_sweep_plane_kz.argtypes = [P]
     L.aphid_gpu_sweep_pass_config.argtypes = [P]
+    L.aphid_gpu_sweep_tile_shape.argtypes = [P]
     _lib = L
     return L
 
@@ -422,6 +423,11 @@ class Solver:
         """pipeline configuration of the complex64 pass in use (0: two load
         stages, two blocks per SM for model R; 1: three stages, one block)"""
         return int(self.lib.aphid_gpu_sweep_pass_config(self._h))
+
+    def sweep_tile_shape(self):
+        """plane-tile shape of the fused passes in use (0: 16 x 16 nodes,
+        1: 32 x 8)"""
+        return int(self.lib.aphid_gpu_sweep_tile_shape(self._h))
 
     def sweep_fetch(self, sys):
         x = np.empty(self.n, np.complex128)

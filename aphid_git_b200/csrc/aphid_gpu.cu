@@ -22,6 +22,7 @@
 
 #include "../../include/aphid_gpu.h"
 #include "aphid_sweep.cuh"
+#include "aphid_apply64.cuh"
 
 using namespace aphid;
 
@@ -43,6 +44,7 @@ struct aphid_ctx {
   GridDev g{};
   Tiles tiles{};
   Tiles ptiles{};  // plane tiles of the complex64 operator pass
+  Tiles atiles{};  // plane tiles of the complex128 operator (k_apply64s)
   NodeLayout nl{};  // node layout of the complex64 sweep state
   int sblk = 0;  // blocks of the streaming kernels
 
@@ -90,7 +92,7 @@ struct aphid_ctx {
   int *sw_work = nullptr;    // [2] work counter of the persistent pass, then [order]
   int *group_work = nullptr; // [2] work counter of group launches led by this context
   int num_sms = 148;         // multiprocessors of the device
-  PassMaps maps{};           // TMA tensor maps of the pass
+  PassMaps maps[kTileShapes]{};  // TMA tensor maps of the fused passes, per tile shape
   int *sw_err = nullptr;     // set by a kernel whose bounded wait gave up
   SweepSys *sw_sys = nullptr;
   double *sw_part = nullptr;
@@ -197,7 +199,10 @@ int ensure_work(aphid_ctx *ctx) {
     ctx->w64 = nullptr;
     return fail(ctx, APHID_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
   }
-  const long long slots = std::max<long long>(ctx->sblk, ctx->tiles.count());
+  const long long slots = std::max<long long>(ctx->sblk, std::max(ctx->tiles.count(), ctx->atiles.count()));
+  CK(cudaFuncSetAttribute(k_apply64s<kApplyPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplyShm));
+  CK(cudaFuncSetAttribute(k_apply64s<kApplyQmr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplyShm));
+  CK(cudaFuncSetAttribute(k_apply64s<kApplyEps>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplyShm));
   CK(cudaMalloc(&ctx->d_sc, sizeof(Scal64)));
   CK(cudaMalloc(&ctx->d_part, (size_t)slots * 3 * sizeof(double)));
   CK(cudaMalloc(&ctx->d_cnt, 16 * sizeof(unsigned)));
@@ -239,8 +244,8 @@ dim3 node_grid(const aphid_ctx *ctx) {
 }
 
 void launch_apply(aphid_ctx *ctx, const double2 *k2, const double2 *in, double2 *out) {
-  k_apply64<kApplyPlain><<<(unsigned)ctx->tiles.count(), kOpThreads, 0, ctx->stream>>>(
-      ctx->g, ctx->tiles, k2, in, out, nullptr, nullptr, nullptr, nullptr);
+  k_apply64s<kApplyPlain><<<(unsigned)ctx->atiles.count(), kAThreads, kApplyShm, ctx->stream>>>(
+      ctx->g, ctx->atiles, k2, in, out, nullptr, nullptr, nullptr, nullptr);
 }
 
 // One QMR iteration (src/aphid_qmr.f90:297-390) as four launches.
@@ -250,8 +255,8 @@ void launch_iteration(aphid_ctx *ctx) {
   double2 *inv = wv(ctx, W_INV), *x = wv(ctx, W_X), *r = wv(ctx, W_R), *s = wv(ctx, W_S);
   double2 *p = wv(ctx, W_P), *d = wv(ctx, W_D), *v = wv(ctx, W_V), *q = wv(ctx, W_Q);
   k_pupd64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, v, inv, p, ctx->d_sc);
-  k_apply64<kApplyQmr><<<(unsigned)ctx->tiles.count(), kOpThreads, 0, ctx->stream>>>(
-      ctx->g, ctx->tiles, wv(ctx, W_K2), p, q, ctx->d_sc, nullptr, ctx->d_part, ctx->d_cnt + 1);
+  k_apply64s<kApplyQmr><<<(unsigned)ctx->atiles.count(), kAThreads, kApplyShm, ctx->stream>>>(
+      ctx->g, ctx->atiles, wv(ctx, W_K2), p, q, ctx->d_sc, nullptr, ctx->d_part, ctx->d_cnt + 1);
   k_rho64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, q, v, ctx->d_sc, ctx->d_part, ctx->d_cnt + 2);
   k_upd64<<<sb, kStreamThreads, 0, ctx->stream>>>(n, p, q, inv, d, x, s, r, v, ctx->d_sc, ctx->d_hist,
                                                   ctx->d_part, ctx->d_cnt + 3);
@@ -421,13 +426,14 @@ int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz, const double *dx,
   ctx->ny = ny;
   ctx->nz = nz;
   ctx->n = n;
-  Tiles t;
+  Tiles t{};
   t.ti = (nx + kTileI - 1) / kTileI;
   t.tj = (ny + kTileJ - 1) / kTileJ;
   const long long cols = (long long)t.ti * t.tj;
   t.kz = (int)std::min<long long>(32, std::max<long long>(1, cols * nz / (148 * 8)));
   t.tk = (nz + t.kz - 1) / t.kz;
   ctx->tiles = t;
+  ctx->atiles = apply_tiles(nx, ny, nz, ctx->num_sms);
   ctx->nl.nxp = (nx + 3) / 4 * 4;
   ctx->nl.N = (long long)ctx->nl.nxp * ny * nz;
   ctx->sblk = (int)std::max<long long>(1, std::min<long long>((n + kStreamThreads - 1) / kStreamThreads, 148 * 8));
@@ -668,11 +674,14 @@ int aphid_gpu_inprod_dev(aphid_ctx *ctx, const void *d_k2, const void *d_in, voi
   int rc = check_ready(ctx);
   if (rc) return rc;
   if (!d_k2 || !d_in || !d_out) return fail(ctx, APHID_ERR_BADARG, "null device pointer");
+  // complex128 values move as 16-byte vectors (loads, stores and cp.async)
+  if (((uintptr_t)d_k2 | (uintptr_t)d_in | (uintptr_t)d_out | (uintptr_t)d_eps) & 15u)
+    return fail(ctx, APHID_ERR_BADARG, "device arrays must be 16-byte aligned");
   if ((rc = ensure_work(ctx))) return rc;
-  const unsigned nb = (unsigned)ctx->tiles.count();
+  const unsigned nb = (unsigned)ctx->atiles.count();
   if (d_eps)
-    k_apply64<kApplyEps><<<nb, kOpThreads, 0, ctx->stream>>>(
-        ctx->g, ctx->tiles, (const double2 *)d_k2, (const double2 *)d_in, (double2 *)d_out, nullptr,
+    k_apply64s<kApplyEps><<<nb, kAThreads, kApplyShm, ctx->stream>>>(
+        ctx->g, ctx->atiles, (const double2 *)d_k2, (const double2 *)d_in, (double2 *)d_out, nullptr,
         (double2 *)d_eps, ctx->d_part, ctx->d_cnt + 8);
   else
     launch_apply(ctx, (const double2 *)d_k2, (const double2 *)d_in, (double2 *)d_out);
@@ -748,8 +757,11 @@ int encode_map(aphid_ctx *ctx, CUtensorMap *m, CUtensorMapDataType type, int ran
 // node along i).  w: q^ and v^ of both buffer sets, 5-D (i, j, k, vector x
 // component = 8, set x system), one box = 20 x 18 nodes of one z-plane, both
 // vectors and four components; p: the p^ ring, 5-D (i, j, k, component, slot
-// x system), one box = the same nodes, four components.
-int inner_maps(aphid_ctx *ctx, CUtensorMap *w, CUtensorMap *p, void *base, int nsys, int ring, int xs) {
+// x system), one box = the same nodes, four components.  Boxes of tile shape
+// TS (20 x 18 or 36 x 10 nodes).
+template <int TS>
+int inner_maps_t(aphid_ctx *ctx, CUtensorMap *w, CUtensorMap *p, void *base, int nsys, int ring, int xs) {
+  constexpr int kPW = PT<TS>::W, kPH = PT<TS>::H;
   const NodeLayout &L = ctx->nl;
   const cuuint64_t es = 8 * (cuuint64_t)xs;  // bytes per node and component
   const cuuint64_t dims[5] = {(cuuint64_t)xs * L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz, 8,
@@ -767,21 +779,38 @@ int inner_maps(aphid_ctx *ctx, CUtensorMap *w, CUtensorMap *p, void *base, int n
   const cuuint32_t pbox[5] = {(cuuint32_t)(xs * kPW), kPH, 1, 4, 1};
   return encode_map(ctx, p, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, (double *)base + 4 * vec, pdims, pstrides, pbox);
 }
+// both tile shapes: complex64 (xs = 1, maps w, p) or complex128 (xs = 2, w64, p64)
+int inner_maps(aphid_ctx *ctx, void *base, int nsys, int ring, int xs) {
+  int rc;
+  for (int ts = 0; ts < kTileShapes; ts++) {
+    PassMaps &M = ctx->maps[ts];
+    CUtensorMap *w = xs == 1 ? &M.w : &M.w64, *p = xs == 1 ? &M.p : &M.p64;
+    if ((rc = ts ? inner_maps_t<1>(ctx, w, p, base, nsys, ring, xs) : inner_maps_t<0>(ctx, w, p, base, nsys, ring, xs)))
+      return rc;
+  }
+  return APHID_OK;
+}
 
-// sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18
-// (one box holds the four components of one model copy; copies follow each
-// other along the component dimension)
+// sigma-bar / eps-bar: 4-D (i, j, k, component) FP32, box 24 x 18 or 40 x 10
+// per tile shape (one box holds the four components of one model copy;
+// copies follow each other along the component dimension)
 int model_maps(aphid_ctx *ctx) {
   const NodeLayout &L = ctx->nl;
   const cuuint64_t dims[4] = {(cuuint64_t)L.nxp, (cuuint64_t)ctx->ny, (cuuint64_t)ctx->nz,
                               4 * (cuuint64_t)std::max(1, ctx->model_copies)};
   const cuuint64_t strides[3] = {(cuuint64_t)L.nxp * 4, (cuuint64_t)L.nxp * ctx->ny * 4, (cuuint64_t)L.N * 4};
-  const cuuint32_t box[4] = {kKW, kPH, 1, 4};
-  int rc = encode_map(ctx, &ctx->maps.sig, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->d_sig32, dims, strides, box);
-  if (rc) return rc;
-  if (ctx->d_epsr32)
-    return encode_map(ctx, &ctx->maps.eps, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->d_epsr32, dims, strides, box);
-  ctx->maps.eps = ctx->maps.sig;  // unused without eps-bar
+  for (int ts = 0; ts < kTileShapes; ts++) {
+    PassMaps &M = ctx->maps[ts];
+    const cuuint32_t box[4] = {(cuuint32_t)(ts ? PT<1>::KW : PT<0>::KW), (cuuint32_t)(ts ? PT<1>::H : PT<0>::H), 1, 4};
+    int rc = encode_map(ctx, &M.sig, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->d_sig32, dims, strides, box);
+    if (rc) return rc;
+    if (ctx->d_epsr32) {
+      if ((rc = encode_map(ctx, &M.eps, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->d_epsr32, dims, strides, box)))
+        return rc;
+    } else {
+      M.eps = M.sig;  // unused without eps-bar
+    }
+  }
   return APHID_OK;
 }
 
@@ -838,20 +867,30 @@ constexpr int kMinKz = 4;  // shallowest z-slab of the complex64 pass
 // z-slab depth when neither the caller nor the tuner chose one: about two
 // work items per SM over the whole batch
 int default_kz(const aphid_ctx *ctx, int nsys) {
+  constexpr int kPTI = PT<0>::I, kPTJ = PT<0>::J;
   const long long cols = (long long)((ctx->nx + kPTI - 1) / kPTI) * ((ctx->ny + kPTJ - 1) / kPTJ) * nsys;
   return (int)std::min<long long>(32, std::max<long long>(kMinKz, cols * ctx->nz / (2LL * ctx->num_sms)));
 }
 
-// plane tiles of the complex64 pass for z-slab depth kz, the work counter
-// and the order in which the pass takes its tiles: most live nodes first, so
-// that the tiles at the far x and y faces (one live column or row on meshes
-// of 16k+1 nodes) fill the tail
-int plane_tiles(aphid_ctx *ctx, int kz) {
-  Tiles tp;
-  tp.ti = (ctx->nx + kPTI - 1) / kPTI;
-  tp.tj = (ctx->ny + kPTJ - 1) / kPTJ;
+// plane tiles of shape ts (see PT) for z-slab depth kz
+Tiles plane_tile_grid(const aphid_ctx *ctx, int kz, int ts) {
+  const int I = ts ? PT<1>::I : PT<0>::I, J = ts ? PT<1>::J : PT<0>::J;
+  Tiles tp{};
+  tp.ti = (ctx->nx + I - 1) / I;
+  tp.tj = (ctx->ny + J - 1) / J;
   tp.kz = std::max(kMinKz, std::min(kz, ctx->nz));
   tp.tk = (ctx->nz + tp.kz - 1) / tp.kz;
+  tp.ts = ts;
+  return tp;
+}
+
+// plane tiles of the fused passes (shape ts, z-slab depth kz), the work
+// counter and the order in which the passes take their tiles: most live nodes
+// first, so that the tiles at the far x and y faces (one live column or row on
+// meshes of 16k+1 nodes) fill the tail
+int plane_tiles(aphid_ctx *ctx, int kz, int ts) {
+  const Tiles tp = plane_tile_grid(ctx, kz, ts);
+  const int kPTI = ts ? PT<1>::I : PT<0>::I, kPTJ = ts ? PT<1>::J : PT<0>::J;
   const long long T = tp.count();
   std::vector<int> order(T);
   std::vector<long long> live(T);
@@ -922,14 +961,12 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     }
     ctx->sw_bps = (int)std::max<long long>(
         1, std::min<long long>((ctx->n + kStreamThreads - 1) / kStreamThreads, std::max(4, 148 * 8 / nsys)));
-    // partial-sum slots for the shallowest slab the tuner may choose
-    Tiles t4;
-    t4.ti = (ctx->nx + kPTI - 1) / kPTI;
-    t4.tj = (ctx->ny + kPTJ - 1) / kPTJ;
-    t4.kz = kMinKz;
-    t4.tk = (ctx->nz + kMinKz - 1) / kMinKz;
-    ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()), t4.count());
-    int rc = plane_tiles(ctx, ctx->plane_kz > 0 ? ctx->plane_kz : default_kz(ctx, nsys));
+    // partial-sum slots for the shallowest slab the tuner may choose, in
+    // either tile shape
+    ctx->sw_slots = std::max<long long>(std::max<long long>(ctx->sw_bps, ctx->tiles.count()),
+                                        std::max(plane_tile_grid(ctx, kMinKz, 0).count(),
+                                                 plane_tile_grid(ctx, kMinKz, 1).count()));
+    int rc = plane_tiles(ctx, ctx->plane_kz > 0 ? ctx->plane_kz : default_kz(ctx, nsys), 0);
     if (rc) return rc;
     CK(cudaMalloc(&ctx->sw_sys, (size_t)nsys * sizeof(SweepSys)));
     CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * kParts * sizeof(double)));
@@ -957,7 +994,7 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     }
     if (!ctx->sw_err) CK(cudaMalloc(&ctx->sw_err, sizeof(int)));
     ctx->sw_f32_ok = true;
-    int rc = inner_maps(ctx, &ctx->maps.w, &ctx->maps.p, ctx->sw_f32, ctx->sw_nsys, ring, 1);
+    int rc = inner_maps(ctx, ctx->sw_f32, ctx->sw_nsys, ring, 1);
     if (rc) return rc;
   }
   return APHID_OK;
@@ -988,7 +1025,7 @@ int sweep_alloc64(aphid_ctx *ctx, int k) {
   }
   if (!ctx->sw_err) CK(cudaMalloc(&ctx->sw_err, sizeof(int)));
   ctx->sw_nsys64 = k;
-  return inner_maps(ctx, &ctx->maps.w64, &ctx->maps.p64, ctx->sw_w64, k, ring, 2);
+  return inner_maps(ctx, ctx->sw_w64, k, ring, 2);
 }
 
 // Sources (gen_rhs, src/aphid.f90:534-743) as sparse (index, value) lists
@@ -1054,78 +1091,86 @@ static __global__ void k_sw_scatter(long long cnt, const long long *__restrict__
   if (t < cnt) b[idx[t]] = make_double2(val[t], 0.0);
 }
 
+// shared memory and resident blocks per SM of the complex64 pass instance
+// for D (eps-bar, tile shape D.tp.ts) in pipeline configuration cfg
+template <int CFG, int TS>
+size_t pass_shm_t(const SweepDev &D) {
+  return D.epsr32 ? PassShm<true, CFG, TS>::bytes : PassShm<false, CFG, TS>::bytes;
+}
 size_t pass_shm(const SweepDev &D, int cfg) {
-  return D.epsr32 ? (cfg ? PassShm<true, 1>::bytes : PassShm<true, 0>::bytes)
-                  : (cfg ? PassShm<false, 1>::bytes : PassShm<false, 0>::bytes);
+  return D.tp.ts ? (cfg ? pass_shm_t<1, 1>(D) : pass_shm_t<0, 1>(D)) : (cfg ? pass_shm_t<1, 0>(D) : pass_shm_t<0, 0>(D));
 }
 int pass_blocks(const SweepDev &D, int cfg) {
-  return D.epsr32 ? (cfg ? PassShm<true, 1>::blocks : PassShm<true, 0>::blocks)
-                  : (cfg ? PassShm<false, 1>::blocks : PassShm<false, 0>::blocks);
+  return (D.epsr32 || cfg) ? 1 : PassShm<false, 0, 0>::blocks;
 }
+static_assert(PassShm<false, 0, 0>::blocks == PassShm<false, 0, 1>::blocks &&
+                  PassShm<true, 0, 0>::blocks == 1 && PassShm<false, 1, 1>::blocks == 1,
+              "pass_blocks: the resident blocks depend on eps-bar and the configuration only");
 
-// opt in to the dynamic shared memory of the pass (once per context)
+// opt in to the dynamic shared memory of the passes (once per context)
+template <int CFG, int TS>
+int pass_attrs_t(aphid_ctx *ctx) {
+  const int r = (int)PassShm<false, CFG, TS>::bytes, e = (int)PassShm<true, CFG, TS>::bytes;
+  CK(cudaFuncSetAttribute(k_sw_pass<false, CFG, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, r));
+  CK(cudaFuncSetAttribute(k_sw_pass<true, CFG, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
+  CK(cudaFuncSetAttribute(k_sw_pass_group<false, CFG, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, r));
+  CK(cudaFuncSetAttribute(k_sw_pass_group<true, CFG, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, e));
+  if (CFG == 0) {
+    const int f = (int)Pass64Shm<TS>::bytes;
+    CK(cudaFuncSetAttribute(k_sw_pass64<false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
+    CK(cudaFuncSetAttribute(k_sw_pass64<true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
+  }
+  return APHID_OK;
+}
 int pass_attrs(aphid_ctx *ctx) {
-  const int r0 = (int)PassShm<false, 0>::bytes, e0 = (int)PassShm<true, 0>::bytes;
-  const int r1 = (int)PassShm<false, 1>::bytes, e1 = (int)PassShm<true, 1>::bytes;
-  CK(cudaFuncSetAttribute(k_sw_pass<false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, r0));
-  CK(cudaFuncSetAttribute(k_sw_pass<false, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, r0));
-  CK(cudaFuncSetAttribute(k_sw_pass<true, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, e0));
-  CK(cudaFuncSetAttribute(k_sw_pass<true, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, e0));
-  CK(cudaFuncSetAttribute(k_sw_pass<false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, r1));
-  CK(cudaFuncSetAttribute(k_sw_pass<false, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, r1));
-  CK(cudaFuncSetAttribute(k_sw_pass<true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, e1));
-  CK(cudaFuncSetAttribute(k_sw_pass<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, e1));
-  const int f = (int)kPass64Shm;
-  CK(cudaFuncSetAttribute(k_sw_pass64<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
-  CK(cudaFuncSetAttribute(k_sw_pass64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
-  CK(cudaFuncSetAttribute(k_sw_pass64<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
-  CK(cudaFuncSetAttribute(k_sw_pass64<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f));
+  int rc;
+  if ((rc = pass_attrs_t<0, 0>(ctx)) || (rc = pass_attrs_t<1, 0>(ctx))) return rc;
+  if ((rc = pass_attrs_t<0, 1>(ctx)) || (rc = pass_attrs_t<1, 1>(ctx))) return rc;
   return APHID_OK;
 }
 
-template <int CFG>
-void launch_pass_cfg(aphid_ctx *ctx, const SweepDev &D, bool timing, unsigned sp, size_t shm) {
-  if (D.epsr32) {
-    if (timing)
-      k_sw_pass<true, true, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
-    else
-      k_sw_pass<true, false, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
-  } else {
-    if (timing)
-      k_sw_pass<false, true, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
-    else
-      k_sw_pass<false, false, CFG><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps);
-  }
+template <int CFG, int TS>
+void launch_pass_t(aphid_ctx *ctx, const SweepDev &D, unsigned sp, size_t shm) {
+  if (D.epsr32)
+    k_sw_pass<true, CFG, TS><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps[TS]);
+  else
+    k_sw_pass<false, CFG, TS><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps[TS]);
 }
 
-// persistent: PassShm<EPS, CFG>::blocks resident blocks per SM, in the
-// pipeline configuration the tuner chose (ctx->pass_cfg)
-void launch_pass(aphid_ctx *ctx, const SweepDev &D, bool timing) {
+// persistent: PassShm::blocks resident blocks per SM, in the pipeline
+// configuration the tuner chose (ctx->pass_cfg), over the tiles of D.tp;
+// timing: a timing launch (SweepDev::timing)
+void launch_pass(aphid_ctx *ctx, const SweepDev &D0, bool timing) {
+  SweepDev D = D0;
+  D.timing = timing ? 1 : 0;
   const long long items = D.tp.count() * D.nsys;
   const int cfg = ctx->pass_cfg;
   const unsigned sp = (unsigned)std::min<long long>(items, (long long)pass_blocks(D, cfg) * ctx->num_sms);
   const size_t shm = pass_shm(D, cfg);
-  if (cfg)
-    launch_pass_cfg<1>(ctx, D, timing, sp, shm);
+  if (D.tp.ts)
+    cfg ? launch_pass_t<1, 1>(ctx, D, sp, shm) : launch_pass_t<0, 1>(ctx, D, sp, shm);
   else
-    launch_pass_cfg<0>(ctx, D, timing, sp, shm);
+    cfg ? launch_pass_t<1, 0>(ctx, D, sp, shm) : launch_pass_t<0, 0>(ctx, D, sp, shm);
 }
 
 // the complex128 pass, persistent like launch_pass
-void launch_pass64(aphid_ctx *ctx, const SweepDev &D, bool timing) {
+template <int TS>
+void launch_pass64_t(aphid_ctx *ctx, const SweepDev &D, unsigned sp) {
+  const size_t shm = Pass64Shm<TS>::bytes;
+  if (D.epsr64)
+    k_sw_pass64<true, TS><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps[TS]);
+  else
+    k_sw_pass64<false, TS><<<sp, kPThreads, shm, ctx->stream>>>(D, ctx->maps[TS]);
+}
+void launch_pass64(aphid_ctx *ctx, const SweepDev &D0, bool timing) {
+  SweepDev D = D0;
+  D.timing = timing ? 1 : 0;
   const long long items = D.tp.count() * D.nsys;
   const unsigned sp = (unsigned)std::min<long long>(items, (long long)ctx->num_sms);
-  if (D.epsr64) {
-    if (timing)
-      k_sw_pass64<true, true><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
-    else
-      k_sw_pass64<true, false><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
-  } else {
-    if (timing)
-      k_sw_pass64<false, true><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
-    else
-      k_sw_pass64<false, false><<<sp, kPThreads, kPass64Shm, ctx->stream>>>(D, ctx->maps);
-  }
+  if (D.tp.ts)
+    launch_pass64_t<1>(ctx, D, sp);
+  else
+    launch_pass64_t<0>(ctx, D, sp);
 }
 
 // One graph round: flush the pending solution updates (this ends the inner
@@ -1182,9 +1227,10 @@ int sweep_graph(aphid_ctx *ctx, const SweepDev &D, bool fused64) {
 // and a hash of its name, so ranks on different GPU models keep their own
 // choices.
 typedef std::array<int, 7> TuneKey;  // nx, ny, nz, nsys, eps-bar present + 2 x complex128 pass, SMs, name hash
-// A tuned choice: z-slab depth kz and pipeline configuration cfg of the pass
+// A tuned choice: z-slab depth kz, pipeline configuration cfg (complex64
+// pass) and tile shape ts of the pass
 struct Tuned {
-  int kz = 0, cfg = 0;
+  int kz = 0, cfg = 0, ts = 0;
 };
 
 
@@ -1205,14 +1251,14 @@ Tuned tune_file_lookup(const TuneKey &k) {
   if (!f) return found;
   char line[256];
   while (std::fgets(line, sizeof line, f)) {
-    int v[9];
+    int v[10];
     char tail;
-    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %c", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7],
-                    &v[8], &tail) != 9)
+    if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %c", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6],
+                    &v[7], &v[8], &v[9], &tail) != 10)
       continue;  // torn, foreign or old-format record
-    bool same = v[7] >= kMinKz && (v[8] == 0 || v[8] == 1);
+    bool same = v[7] >= kMinKz && (v[8] == 0 || v[8] == 1) && v[9] >= 0 && v[9] < kTileShapes;
     for (int q = 0; q < 7; q++) same = same && v[q] == k[q];
-    if (same) found = Tuned{v[7], v[8]};
+    if (same) found = Tuned{v[7], v[8], v[9]};
   }
   std::fclose(f);
   return found;
@@ -1222,8 +1268,8 @@ void tune_file_store(const TuneKey &k, Tuned t) {
   const char *path = std::getenv("APHID_TUNE_CACHE");
   if (!path || !*path) return;
   char line[160];
-  const int len = std::snprintf(line, sizeof line, "%d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4], k[5],
-                                k[6], t.kz, t.cfg);
+  const int len = std::snprintf(line, sizeof line, "%d %d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4],
+                                k[5], k[6], t.kz, t.cfg, t.ts);
   if (len <= 0 || len >= (int)sizeof line) return;
   const int fd = ::open(path, O_WRONLY | O_APPEND | O_CREAT, 0644);
   if (fd < 0) return;
@@ -1246,9 +1292,10 @@ void device_identity(const aphid_ctx *ctx, int &sms, int &name_hash) {
   name_hash = (int)(h & 0x7fffffff);
 }
 
-// The complex64 pass is timed for every (kz, cfg): the z-slab depths and the
-// two pipeline configurations of PassShm (two stages with two blocks per SM
-// for model R, or three stages in one); the complex128 pass for kz alone.
+// The complex64 pass is timed for every (ts, cfg, kz): the two tile shapes of
+// PT, the two pipeline configurations of PassShm (two stages with two blocks
+// per SM for model R, or three stages in one) and the z-slab depths; the
+// complex128 pass for (ts, kz).
 int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
   int sms, name_hash;
   device_identity(ctx, sms, name_hash);
@@ -1268,6 +1315,7 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
     CK(cudaMemsetAsync(ctx->sw_err, 0, sizeof(int), ctx->stream));
     float best_ms = 0.f;
     const int cand[] = {4, 6, 8, 12, 16, 24, 32};
+    for (int ts = 0; ts < kTileShapes; ts++)
     for (int cfg = 0; cfg < (fused ? 1 : 2); cfg++) {
       int last_tk = -1;
       for (int c : cand) {
@@ -1275,7 +1323,7 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
         const int tk = (ctx->nz + c - 1) / c;
         if (tk == last_tk) continue;  // same slabs as the previous candidate
         last_tk = tk;
-        if ((rc = plane_tiles(ctx, c))) return rc;
+        if ((rc = plane_tiles(ctx, c, ts))) return rc;
         ctx->pass_cfg = cfg;
         SweepDev D = sweep_dev(ctx, nsys);
         D.tmix = 0.f;
@@ -1294,17 +1342,18 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         if (!best.kz || ms < best_ms) {
-          best = Tuned{c, cfg};
+          best = Tuned{c, cfg, ts};
           best_ms = ms;
         }
         if (ctx->verbose)
-          std::fprintf(stderr, "aphid_gpu: tune kz=%d cfg=%d %.3f ms/pass%s\n", c, cfg, ms / 5, fused ? " (c128)" : "");
+          std::fprintf(stderr, "aphid_gpu: tune ts=%d kz=%d cfg=%d %.3f ms/pass%s\n", ts, c, cfg, ms / 5,
+                       fused ? " (c128)" : "");
       }
     }
     int kerr = 0;
     CK(cudaMemcpy(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (kerr) return fail(ctx, APHID_ERR_CUDA, "tuner: a tensor-copy wait in the pass timed out");
-    if (!best.kz) best = Tuned{default_kz(ctx, nsys), 0};
+    if (!best.kz) best = Tuned{default_kz(ctx, nsys), 0, 0};
     tune_file_store(key, best);
   }
   {
@@ -1312,8 +1361,8 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
     tune_cache()[key] = best;
   }
   if (!fused) ctx->pass_cfg = best.cfg;
-  if (ctx->ptiles.kz != best.kz || !ctx->sw_work) {
-    if ((rc = plane_tiles(ctx, best.kz))) return rc;
+  if (ctx->ptiles.kz != best.kz || ctx->ptiles.ts != best.ts || !ctx->sw_work) {
+    if ((rc = plane_tiles(ctx, best.kz, best.ts))) return rc;
   }
   return APHID_OK;
 }
@@ -1710,7 +1759,8 @@ int sweep_prepare(aphid_ctx *ctx, int nsys, const double *omega, const int *sour
   }
   if (mixed || fused) {
     if (ctx->plane_kz > 0) {
-      if (ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) && (rc = plane_tiles(ctx, ctx->plane_kz)))
+      if ((ctx->ptiles.kz != std::max(kMinKz, std::min(ctx->plane_kz, ctx->nz)) || ctx->ptiles.ts != 0) &&
+          (rc = plane_tiles(ctx, ctx->plane_kz, 0)))
         return rc;
     } else if (mixed && (rc = tune_kz(ctx, nsys, false))) {  // FUSED64 tunes per chunk in run_fused
       return rc;
@@ -1834,6 +1884,24 @@ int sweep_finish(aphid_ctx *ctx, SweepPrep &P, const double *omega, const aphid_
   return APHID_OK;
 }
 
+template <bool EPS, int CFG, int TS>
+void launch_group_t(unsigned grid, size_t shm, cudaStream_t st, const PassGroup &G) {
+  k_sw_pass_group<EPS, CFG, TS><<<grid, kPThreads, shm, st>>>(G);
+}
+void launch_group(bool eps, int cfg, int ts, unsigned grid, size_t shm, cudaStream_t st, const PassGroup &G) {
+  if (eps) {
+    if (ts)
+      cfg ? launch_group_t<true, 1, 1>(grid, shm, st, G) : launch_group_t<true, 0, 1>(grid, shm, st, G);
+    else
+      cfg ? launch_group_t<true, 1, 0>(grid, shm, st, G) : launch_group_t<true, 0, 0>(grid, shm, st, G);
+  } else {
+    if (ts)
+      cfg ? launch_group_t<false, 1, 1>(grid, shm, st, G) : launch_group_t<false, 0, 1>(grid, shm, st, G);
+    else
+      cfg ? launch_group_t<false, 1, 0>(grid, shm, st, G) : launch_group_t<false, 0, 0>(grid, shm, st, G);
+  }
+}
+
 // Several contexts' complex64 sweeps as one: per graph round every context's
 // flush and outer step, then graph_iters launches of k_sw_pass_group, whose
 // persistent blocks take the work items of all meshes from one counter, with
@@ -1860,6 +1928,20 @@ int run_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opt
   aphid_ctx *ctx = c0;  // CK reports on the first context
   const cudaStream_t st = c0->stream;
   const bool eps = c0->d_epsr32 != nullptr;
+  // one kernel instance serves all meshes: the tile shape of the first
+  // context's tuned choice for every one
+  const int ts = c0->ptiles.ts;
+  for (int a = 1; a < njob; a++) {
+    aphid_ctx *c = jobs[a].ctx;
+    if (c->ptiles.ts == ts) continue;
+    if ((rc = plane_tiles(c, c->ptiles.kz, ts))) {
+      for (auto &q : P) q.release();
+      return rc;
+    }
+    P[a].D.tp = c->ptiles;
+    P[a].D.work = c->sw_work;
+    P[a].D.order = c->sw_work + 2;
+  }
   // items of every mesh, the larger meshes first
   std::vector<int> ord(njob);
   for (int a = 0; a < njob; a++) ord[a] = a;
@@ -1872,7 +1954,7 @@ int run_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opt
   for (int q = 0; q < njob; q++) {
     const int a = ord[q];
     G.D[q] = P[a].D;
-    G.M[q] = jobs[a].ctx->maps;
+    G.M[q] = jobs[a].ctx->maps[ts];
     G.first[q + 1] = G.first[q] + P[a].D.tp.count() * P[a].D.nsys;
     ring = std::min(ring, P[a].D.ring);
   }
@@ -1886,12 +1968,6 @@ int run_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opt
   const int cfg = c0->pass_cfg;
   const int per_sm = pass_blocks(P[0].D, cfg);
   const size_t shm = pass_shm(P[0].D, cfg);
-  if (eps)
-    CK(cudaFuncSetAttribute(cfg ? k_sw_pass_group<true, false, 1> : k_sw_pass_group<true, false, 0>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-  else
-    CK(cudaFuncSetAttribute(cfg ? k_sw_pass_group<false, false, 1> : k_sw_pass_group<false, false, 0>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
   const unsigned grid = (unsigned)std::min<long long>(G.first[njob], (long long)per_sm * c0->num_sms);
   for (int a = 0; a < njob; a++) {
     aphid_ctx *c = jobs[a].ctx;
@@ -1918,17 +1994,7 @@ int run_group(int njob, const aphid_group_job *jobs, const aphid_sweep_opts *opt
     k_sw_resid<float2><<<(unsigned)(D.t.count() * D.nsys), kOpThreads, 0, st>>>(D);
   }
   for (int it = 0; it < c0->graph_iters; it++) {
-    if (eps) {
-      if (cfg)
-        k_sw_pass_group<true, false, 1><<<grid, kPThreads, shm, st>>>(G);
-      else
-        k_sw_pass_group<true, false, 0><<<grid, kPThreads, shm, st>>>(G);
-    } else {
-      if (cfg)
-        k_sw_pass_group<false, false, 1><<<grid, kPThreads, shm, st>>>(G);
-      else
-        k_sw_pass_group<false, false, 0><<<grid, kPThreads, shm, st>>>(G);
-    }
+    launch_group(eps, cfg, ts, grid, shm, st, G);
     if ((it + 1) % ring == 0) flush();
   }
   for (int a = 0; a < njob; a++) {
@@ -2160,6 +2226,11 @@ int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx) {
 int aphid_gpu_sweep_pass_config(aphid_ctx *ctx) {
   if (!ctx) return APHID_ERR_BADARG;
   return ctx->pass_cfg;
+}
+
+int aphid_gpu_sweep_tile_shape(aphid_ctx *ctx) {
+  if (!ctx) return APHID_ERR_BADARG;
+  return ctx->ptiles.ts;
 }
 
 int aphid_gpu_sweep_apply(aphid_ctx *ctx, const aphid_z *x, aphid_z *y) {

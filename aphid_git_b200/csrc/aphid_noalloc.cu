@@ -116,7 +116,7 @@ extern "C" int aphid_gpu_inprod_eps_noalloc(int nx, int ny, int nz, const double
   g.n = g.op + (long long)nx * ny * nz;
 
   // tiles bounded by the scratch's partial-sum slots
-  Tiles t;
+  Tiles t{};
   t.ti = (nx + kTileI - 1) / kTileI;
   t.tj = (ny + kTileJ - 1) / kTileJ;
   const long long cols = (long long)t.ti * t.tj;  // <= 32 * 256 < kMaxSlots

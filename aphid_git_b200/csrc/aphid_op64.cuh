@@ -21,6 +21,7 @@ constexpr int kTileI = 32, kTileJ = 4, kOpThreads = kTileI * kTileJ;
 
 struct Tiles {
   int ti, tj, tk, kz;
+  int ts;  // shape of the plane tiles of the fused passes (0: 16 x 16, 1: 32 x 8); 0 for column tiles
   __host__ __device__ long long count() const { return (long long)ti * tj * tk; }
 };
 

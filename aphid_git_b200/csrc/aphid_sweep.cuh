@@ -103,6 +103,14 @@ constexpr int kStallWindow = 400;
 // Heterogeneous land models stay above 1e-5.
 constexpr double kDeltaFloor = 1e-6;
 constexpr int kStEscalated = 4;
+// A complex64 cycle that lowers the FP64 residual by less than this factor is
+// slow; with escalation on, kSlowCycles slow cycles in a row also end the
+// system with kStEscalated.  Restarted complex64 cycles can keep stalling at
+// the plateau of an unrestarted recurrence (sweep meshes with km cells at
+// 1e-3 Hz: 35 cycles in 20000 iterations without reaching 1e-8, while
+// complex128 converges) without the bilinear form ever collapsing.
+constexpr double kSlowCycle = 0.5;
+constexpr int kSlowCycles = 2;
 // longest pending-update list (the p^ ring has up to kMaxRing + 1 slots)
 constexpr int kMaxRing = 8;
 
@@ -127,15 +135,26 @@ struct SweepSys {
   int stall_window;          // window length (INT_MAX: no stall test)
   int escalate;              // 1: end with kStEscalated when the bilinear form collapses
   int escalated;             // set by the pass; the outer step then ends the system
+  int slow;                  // slow cycles in a row (see kSlowCycle)
+  double rprev;              // FP64 residual norm at the previous outer step
   double mon_level;          // the monitor runs once the predicted true residual is below this x ||b||
 };
 
-// plane tile of the complex64 pass: 16 x 16 nodes marching along k; staged
-// planes cover i0-2 .. i0+17 (20, even start: 16-byte TMA x origin) and
-// j0-1 .. j0+16 (18); sigma-bar planes cover i0-4 .. i0+19 (24).
-constexpr int kPTI = 16, kPTJ = 16, kPThreads = kPTI * kPTJ;
-constexpr int kPW = kPTI + 4, kPH = kPTJ + 2, kPN = kPW * kPH;   // 20 x 18
-constexpr int kKW = kPTI + 8, kKN = kKW * kPH;                    // 24 x 18
+// Plane tiles of the fused passes, marching along k, in two shapes that the
+// autotuner chooses between: TS 0, 16 x 16 nodes (the smallest halo; fastest
+// for one system) and TS 1, 32 x 8 (36-node staged rows of 288 B in
+// complex64; fastest for large batches, 16.0 against 19.0 ms per pass over 24
+// systems of 50.8 M unknowns).  Staged planes cover i0-2 .. i0+I+1 (even
+// start: 16-byte TMA x origin) and j0-1 .. j0+J; sigma-bar planes cover
+// i0-4 .. i0+I+3.  256 threads, one per node of the tile.
+template <int TS>
+struct PT {
+  static constexpr int I = TS ? 32 : 16, J = TS ? 8 : 16;
+  static constexpr int W = I + 4, H = J + 2, N = W * H;  // staged plane: 20 x 18 or 36 x 10
+  static constexpr int KW = I + 8, KN = KW * H;          // sigma-bar plane: 24 x 18 or 40 x 10
+};
+constexpr int kPThreads = 256, kTileShapes = 2;
+static_assert(PT<0>::I * PT<0>::J == kPThreads && PT<1>::I * PT<1>::J == kPThreads, "one thread per tile node");
 
 struct NodeLayout {
   int nxp;      // padded row length (multiple of 4)
@@ -146,7 +165,7 @@ struct SweepDev {
   GridDev g;
   NodeLayout L;
   Tiles t;   // 32 x 4 column tiles (complex128 residual passes)
-  Tiles tp;  // 16 x 16 plane tiles (complex64 pass)
+  Tiles tp;  // plane tiles of the fused passes (shape tp.ts, see PT)
   long long n;           // unknowns per system (reference layout)
   int nsys, bps;         // systems; blocks per system of the pointwise kernels
   long long slots;       // partial-sum slots per system
@@ -169,6 +188,7 @@ struct SweepDev {
   int *ndone;
   int *err;                      // set when a bounded wait gives up
   float tmix;                    // 1; 0 in timing launches (d^, x^ rewritten unchanged)
+  int timing;                    // fused passes: 1 in timing launches (see k_sw_pass)
   int *work;                     // [2]: next work item, blocks finished (complex64 pass)
   const int *order;              // plane tiles in the order the pass takes them
   // complex128 inner storage (k_sw_pass64): same layouts, double2
@@ -847,11 +867,13 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_resid(SweepDev D) {
       S->rnorm = sqrt(tot.v[0]);
       S->has_inner = 0;
       S->npend = 0;  // flushed by k_sw_dxupd before this step
+      S->slow = (S->outer_it > 0 && S->rnorm > kSlowCycle * S->rprev) ? S->slow + 1 : 0;
+      S->rprev = S->rnorm;
       if (!isfinite(S->rnorm)) {
         mark_done(D, S, 3);
       } else if (S->rnorm < S->target * S->bnorm) {
         mark_done(D, S, 0);
-      } else if (S->escalated) {
+      } else if (S->escalated || (S->escalate && S->slow >= kSlowCycles)) {
         mark_done(D, S, kStEscalated);
       } else if (S->outer_it >= S->max_outer || S->total_it >= S->max_it) {
         mark_done(D, S, 1);
@@ -982,25 +1004,25 @@ struct PassMaps {
   CUtensorMap p64;       // complex128 p^ ring: 5-D (2 nxp, ny, nz, 4, slot x system), 8-byte elements
 };
 
-constexpr unsigned kVecPlane = kPN * 8u;         // one component of one vector, one staged plane
-constexpr unsigned kRawBytes = 12u * kVecPlane;  // q^, v^, p^ with halo, four components each
-constexpr unsigned kSigBytes = 4u * kKN * 4u;    // sigma-bar with halo, four components
-constexpr unsigned kUBytes = 4u * kVecPlane;     // u of one plane
 // Shared memory and occupancy of the pass, in two pipeline configurations
 // that the autotuner chooses between per mesh and batch: CFG 0, two load
 // stages, with two resident blocks per SM for model R (16 warps, at most 128
 // registers per thread); CFG 1, three load stages in one block per SM.
 // Models C, I and D stage eps-bar too and fit one block per SM in both.  Each
 // stage holds q^ v^ (8 components) and p^ (4) of plane m+1 with halo and
-// sigma-bar [eps-bar] of plane m (41.5 KB, 48.4 KB with eps-bar); then two u
-// planes and the mbarriers.
-template <bool EPS, int CFG>
+// sigma-bar [eps-bar] of plane m (16 x 16 tiles: 40.5 KB, 47.3 KB with
+// eps-bar; 32 x 8: 40.0 KB, 46.3 KB); then two u planes and the mbarriers.
+template <bool EPS, int CFG, int TS>
 struct PassShm {
+  static constexpr unsigned vec_plane = PT<TS>::N * 8u;  // one component of one vector, one staged plane
+  static constexpr unsigned raw = 12u * vec_plane;       // q^, v^, p^ with halo, four components each
+  static constexpr unsigned sig_bytes = 4u * PT<TS>::KN * 4u;  // sigma-bar with halo, four components
+  static constexpr unsigned ubytes = 4u * vec_plane;     // u of one plane
   static constexpr int stages = CFG == 0 ? 2 : 3;
   static constexpr int blocks = (EPS || CFG == 1) ? 1 : 2;  // resident blocks per SM
-  static constexpr unsigned sig = kRawBytes;
-  static constexpr unsigned stage = kRawBytes + (EPS ? 2u : 1u) * kSigBytes;
-  static constexpr size_t bytes = stages * (size_t)stage + 2 * (size_t)kUBytes + 128;
+  static constexpr unsigned sig = raw;
+  static constexpr unsigned stage = raw + (EPS ? 2u : 1u) * sig_bytes;
+  static constexpr size_t bytes = stages * (size_t)stage + 2 * (size_t)ubytes + 128;
 };
 constexpr int kWaitTries = 1 << 24;
 
@@ -1173,25 +1195,28 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T, int ring
 // zeros, and pads and absent components are stored zeros, so zero padding
 // reproduces the reference's clamped neighbours (their coefficients are zero
 // at the boundary).
-// EPS: models C, I and D (eps-bar not 1).  TIMING: the same pass over
+// EPS: models C, I and D (eps-bar not 1).  D.timing: the same pass over
 // resident data without the phase test and the scalar step; it flips the
 // buffer set and advances the ring like an iteration does, so consecutive
 // timing launches read what the previous one wrote (d^ and the x64 solution
-// are untouched).
+// are untouched).  A run-time switch rather than a second instance, so that
+// timing launches run the very code (and register allocation) of the solve.
 // One work item (a tile's z-slab of one system) of the complex64 pass, on
 // the mesh and buffers of D with the tensor maps M.  shm: the pass's dynamic
 // shared memory; bar, phase: its stage mbarriers and their wait parities.
-template <bool EPS, bool TIMING, int CFG>
+template <bool EPS, int CFG, int TS>
 __device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, long long item,
                                           unsigned char *shm, unsigned long long *bar, unsigned &phase) {
-  using SH = PassShm<EPS, CFG>;
+  using SH = PassShm<EPS, CFG, TS>;
   constexpr int kStages = SH::stages;
-  constexpr unsigned kStage = SH::stage;
+  constexpr unsigned kStage = SH::stage, kVecPlane = SH::vec_plane, kSigBytes = SH::sig_bytes;
+  constexpr int kPTI = PT<TS>::I, kPTJ = PT<TS>::J, kPW = PT<TS>::W, kPN = PT<TS>::N, kKW = PT<TS>::KW,
+                kKN = PT<TS>::KN;
   float2 *Ub = reinterpret_cast<float2 *>(shm + kStages * kStage);  // [2][4][kPN]
   const int sys = (int)(item % D.nsys);
   const long long tile = __ldg(D.order + item / D.nsys);
   SweepSys *S = D.sys + sys;
-  if (!TIMING && S->phase != PH_INNER) return;
+  if (!D.timing && S->phase != PH_INNER) return;
 
   const GridDev &g = D.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -1441,7 +1466,7 @@ __device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, 
   if (arrive<kParts, kPThreads>(blk, part, cnt, (unsigned)tile, nt)) {
     Vals<kParts> tot = final_reduce<kParts, kPThreads>(part, cnt, nt);
     if (threadIdx.x == 0) {
-      if (TIMING) {
+      if (D.timing) {
         S->cur ^= 1;
         S->pslot = (S->pslot + 1) % (D.ring + 1);
       } else {
@@ -1466,6 +1491,14 @@ __device__ __forceinline__ bool pass_block_init(unsigned char *shm, unsigned lon
   }
   return aligned;
 }
+// the plane tiles of D are of shape TS (the launch picked the instance from
+// them); otherwise the block takes no work and the launch reports the error
+template <int TS>
+__device__ __forceinline__ bool tiles_are(const SweepDev &D, int *err) {
+  if (D.tp.ts == TS) return true;
+  if (threadIdx.x == 0) atomicExch(err, 3);
+  return false;
+}
 // the last block out of a persistent launch re-arms its work counter
 __device__ __forceinline__ void pass_block_done(int *work) {
   if (threadIdx.x == 0) {
@@ -1478,14 +1511,14 @@ __device__ __forceinline__ void pass_block_done(int *work) {
   }
 }
 
-template <bool EPS, bool TIMING, int CFG>
-__global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG>::blocks) k_sw_pass(SweepDev D,
-                                                                                 const __grid_constant__ PassMaps M) {
-  using SH = PassShm<EPS, CFG>;
+template <bool EPS, int CFG, int TS>
+__global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG, TS>::blocks) k_sw_pass(SweepDev D,
+                                                                                     const __grid_constant__ PassMaps M) {
+  using SH = PassShm<EPS, CFG, TS>;
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * kUBytes);
-  const bool aligned = pass_block_init<SH::stages>(shm, bar, D.err);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * SH::ubytes);
+  const bool aligned = pass_block_init<SH::stages>(shm, bar, D.err) && tiles_are<TS>(D, D.err);
   unsigned phase = 0;  // bit q: parity of the next wait on stage q
   const long long total = aligned ? D.tp.count() * D.nsys : 0;
   for (;;) {
@@ -1494,7 +1527,7 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG>::blocks) k_sw_pas
     __syncthreads();
     const long long item = s_item;
     if (item >= total) break;
-    pass_item<EPS, TIMING, CFG>(D, M, item, shm, bar, phase);
+    pass_item<EPS, CFG, TS>(D, M, item, shm, bar, phase);
   }
   pass_block_done(D.work);
 }
@@ -1513,13 +1546,14 @@ struct PassGroup {
   PassMaps M[kMaxGroup];
 };
 
-template <bool EPS, bool TIMING, int CFG>
-__global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG>::blocks) k_sw_pass_group(const __grid_constant__ PassGroup G) {
-  using SH = PassShm<EPS, CFG>;
+template <bool EPS, int CFG, int TS>
+__global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG, TS>::blocks) k_sw_pass_group(const __grid_constant__ PassGroup G) {
+  using SH = PassShm<EPS, CFG, TS>;
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * kUBytes);
-  const bool aligned = pass_block_init<SH::stages>(shm, bar, G.D[0].err);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * SH::ubytes);
+  bool aligned = pass_block_init<SH::stages>(shm, bar, G.D[0].err);
+  for (int m = 0; m < G.n; m++) aligned = aligned && tiles_are<TS>(G.D[m], G.D[0].err);
   unsigned phase = 0;
   const long long total = aligned ? G.first[G.n] : 0;
   for (;;) {
@@ -1530,7 +1564,7 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG>::blocks) k_sw_pas
     if (item >= total) break;
     int m = 0;
     while (m + 1 < G.n && item >= G.first[m + 1]) m++;
-    pass_item<EPS, TIMING, CFG>(G.D[m], G.M[m], item - G.first[m], shm, bar, phase);
+    pass_item<EPS, CFG, TS>(G.D[m], G.M[m], item - G.first[m], shm, bar, phase);
   }
   pass_block_done(G.work);
 }
@@ -1545,9 +1579,12 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG>::blocks) k_sw_pas
 // (pass_scalars); 2 TMA stages of q^ v^ p^ planes (69 KB each); sigma-bar is
 // read with plain loads, prefetched into L1 a plane ahead.
 constexpr int kStages64 = 2;
-constexpr unsigned kRawBytes64 = 12u * kPN * 16u;  // q^, v^, p^ with halo, four components, complex128
-constexpr unsigned kUBytes64 = 4u * kPN * 16u;
-constexpr size_t kPass64Shm = kStages64 * (size_t)kRawBytes64 + 2 * (size_t)kUBytes64 + 128;
+template <int TS>
+struct Pass64Shm {
+  static constexpr unsigned raw = 12u * PT<TS>::N * 16u;  // q^, v^, p^ with halo, four components, complex128
+  static constexpr unsigned ubytes = 4u * PT<TS>::N * 16u;
+  static constexpr size_t bytes = kStages64 * (size_t)raw + 2 * (size_t)ubytes + 128;
+};
 
 // pull a line towards this SM's L1 ahead of its use (no register, no wait)
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
@@ -1619,15 +1656,17 @@ __device__ __forceinline__ double2 node_row64_c(double2 f, double2 fxp, double2 
   return rmul(vol, t);
 }
 
-template <bool EPS, bool TIMING>
+template <bool EPS, int TS>
 __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __grid_constant__ PassMaps M) {
-  constexpr unsigned kStage = kRawBytes64;
+  constexpr unsigned kStage = Pass64Shm<TS>::raw;
+  constexpr int kPTI = PT<TS>::I, kPTJ = PT<TS>::J, kPW = PT<TS>::W, kPN = PT<TS>::N;
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
   double2 *Ub = reinterpret_cast<double2 *>(shm + kStages64 * kStage);  // [2][4][kPN]
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * kUBytes64);
-  const bool aligned = (smem_u32(shm) & 127u) == 0;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * Pass64Shm<TS>::ubytes);
+  bool aligned = (smem_u32(shm) & 127u) == 0;
   if (!aligned && threadIdx.x == 0) atomicExch(D.err, 2);
+  aligned = aligned && tiles_are<TS>(D, D.err);
   if (threadIdx.x == 0 && aligned) {
 #pragma unroll
     for (int q = 0; q < kStages64; q++) mbar_init(smem_u32(&bar[q]));
@@ -1646,7 +1685,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   const int sys = (int)(item % D.nsys);
   const long long tile = __ldg(D.order + item / D.nsys);
   SweepSys *S = D.sys + sys;
-  if (!TIMING && S->phase != PH_INNER) continue;
+  if (!D.timing && S->phase != PH_INNER) continue;
 
   const GridDev &g = D.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -1884,7 +1923,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   if (arrive<kParts, kPThreads>(blk, part, cnt, (unsigned)tile, nt)) {
     Vals<kParts> tot = final_reduce<kParts, kPThreads>(part, cnt, nt);
     if (threadIdx.x == 0) {
-      if (TIMING) {
+      if (D.timing) {
         S->cur ^= 1;
         S->pslot = (S->pslot + 1) % (D.ring64 + 1);
       } else {

@@ -62,8 +62,10 @@ typedef struct aphid_ctx aphid_ctx;
 #define APHID_PREC_MIXED     1   /* complex64 inner QMR inside FP64 defect correction */
 #define APHID_PREC_FUSED64   2   /* complex128 inner QMR, the batched fused pass in FP64 */
 #define APHID_PREC_AUTO      3   /* MIXED; a system whose complex-symmetric Lanczos form
-                                    v^T v collapses below complex64 resolution is finished
-                                    by FUSED64 from its current iterate */
+                                    v^T v collapses below complex64 resolution, or whose
+                                    complex64 cycles twice in a row lower the FP64 residual
+                                    by less than 2x, is finished by FUSED64 from its
+                                    current iterate */
 
 typedef struct {
   int device;        /* CUDA device ordinal */
@@ -182,6 +184,7 @@ int aphid_gpu_qmr_fetch(aphid_ctx *ctx, aphid_z *sol_x, aphid_z *sol_y,
  * When d_eps is non-NULL the bilinear form in^T out (unconjugated, the
  * epsilon of src/aphid_qmr.f90:329) is reduced on the device and written
  * there as one aphid_z.  The reduction uses the context's scratch buffers.
+ * All four pointers must be 16-byte aligned (APHID_ERR_BADARG otherwise).
  * Runs on the context's stream; returns after the launch (asynchronous). */
 int aphid_gpu_inprod_dev(aphid_ctx *ctx, const void *d_k2, const void *d_in,
                          void *d_out, void *d_eps);
@@ -320,6 +323,11 @@ int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx);
  * aphid_opts.plane_kz fixes the depth). */
 int aphid_gpu_sweep_pass_config(aphid_ctx *ctx);
 
+/* Plane-tile shape of the fused passes in use: 0 = 16 x 16 nodes, 1 = 32 x 8;
+ * chosen with the slab depth by the autotuner (0 when aphid_opts.plane_kz
+ * fixes the depth). */
+int aphid_gpu_sweep_tile_shape(aphid_ctx *ctx);
+
 /* Copy system `sys` of the last sweep into x (one [x|y|z|p] vector). */
 int aphid_gpu_sweep_fetch(aphid_ctx *ctx, int sys, aphid_z *x);
 
@@ -351,9 +359,10 @@ int aphid_gpu_sweep_apply(aphid_ctx *ctx, const aphid_z *x, aphid_z *y);
 /* No counterpart in the reference: an addition for callers that cannot call
  * cudaMalloc -- code that runs inside a memory pool or a framework allocator
  * owning all device memory, or a host that must not allocate once a run has
- * started.  It computes the same result as aphid_gpu_inprod_dev with a
- * non-NULL d_eps (out = K in, and the epsilon in^T out written to *d_eps as
- * one aphid_z), but needs no context and allocates nothing: every argument
+ * started.  It computes what aphid_gpu_inprod_dev with a non-NULL d_eps
+ * computes (out = K in, and the epsilon in^T out written to *d_eps as one
+ * aphid_z; the same rows, the epsilon summed in another order), but needs no
+ * context and allocates nothing: every argument
  * is a caller-owned device pointer on the current device (d_dx..d_dzc hold
  * dx(0:n) and dxc(1:n) as in aphid_gpu_set_mesh; d_k2, d_in, d_out are the
  * concatenated [x|y|z|p] complex128 vectors).  Its scratch is one fixed

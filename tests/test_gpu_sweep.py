@@ -345,18 +345,19 @@ def test_autotuner_picks_and_caches_the_slab_depth(tmp_path, monkeypatch):
         X1, i1 = s.sweep(w, src, [0, 0])
         kz = s.sweep_plane_kz()
         cfg = s.sweep_pass_config()
-        assert kz in (4, 6, 8, 12, 16, 24, 32) and kz <= len(zn) and cfg in (0, 1)
+        ts = s.sweep_tile_shape()
+        assert kz in (4, 6, 8, 12, 16, 24, 32) and kz <= len(zn) and cfg in (0, 1) and ts in (0, 1)
         X2, _ = s.sweep(w, src, [0, 0])
         assert s.sweep_plane_kz() == kz          # cached, not retuned
         assert np.array_equal(X1, X2)            # same depth, same bits
     rec = cache.read_text().split()
     sms, name_hash = _device_identity()
-    assert rec[-9:] == [str(v) for v in (18, 17, 26, 2, 0, sms, name_hash, kz, cfg)]
+    assert rec[-10:] == [str(v) for v in (18, 17, 26, 2, 0, sms, name_hash, kz, cfg, ts)]
     with Solver(graph_iters=8, plane_kz=8) as s:
         s.set_nodes(xn, yn, zn)
         s.set_model("R", sig)
         X3, i3 = s.sweep(w, src, [0, 0])
-        assert s.sweep_plane_kz() == 8
+        assert s.sweep_plane_kz() == 8 and s.sweep_tile_shape() == 0
     for a, b, ia, ib in zip(X1, X3, i1, i3):
         assert ia["status_name"] == ib["status_name"] == "converged"
         assert relerr(a, b) < 1e-6
@@ -375,11 +376,13 @@ def _device_identity():
 
 def test_tune_cache_file_is_per_device_and_skips_torn_records(tmp_path, monkeypatch):
     """A record for another device (other SM count) is not used, a torn line
-    is skipped, and this device's record is taken without retuning."""
+    and a record of the older nine-field format are skipped, and this
+    device's record is taken without retuning."""
     sms, name_hash = _device_identity()
     cache = tmp_path / "tune.txt"
-    cache.write_text("15 14 13 1 0 %d %d 16 0\n15 14 13 1 0 %d\n15 14 13 1 0 %d %d 6 1\n"
-                     % (sms + 4, name_hash, sms, sms, name_hash))
+    cache.write_text("15 14 13 1 0 %d %d 16 0 0\n15 14 13 1 0 %d\n15 14 13 1 0 %d %d 8 0\n"
+                     "15 14 13 1 0 %d %d 6 1 1\n"
+                     % (sms + 4, name_hash, sms, sms, name_hash, sms, name_hash))
     monkeypatch.setenv("APHID_TUNE_CACHE", str(cache))
     xn, yn, zn, sig, _ = small_model(seed=12, dims=(15, 14, 13))
     with Solver(graph_iters=8) as s:
@@ -387,8 +390,47 @@ def test_tune_cache_file_is_per_device_and_skips_torn_records(tmp_path, monkeypa
         s.set_model("R", sig)
         _, inf = s.sweep([2 * np.pi], [[("+X", 7, 7, 4)]], [0])
         assert inf[0]["status_name"] == "converged"
-        assert s.sweep_plane_kz() == 6 and s.sweep_pass_config() == 1
-    assert len(cache.read_text().splitlines()) == 3  # taken from the file: nothing appended
+        assert s.sweep_plane_kz() == 6 and s.sweep_pass_config() == 1 and s.sweep_tile_shape() == 1
+    assert len(cache.read_text().splitlines()) == 4  # taken from the file: nothing appended
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fused64"])
+def test_tile_shapes_agree(tmp_path, monkeypatch, precision):
+    """Both plane-tile shapes (16 x 16 and 32 x 8 nodes), forced through the
+    tune cache, on a mesh whose sizes are multiples of neither (the ragged
+    tiles at the far faces) and with three systems: the same operator as the
+    oracle row by row, and solutions of the same sweep that agree within the
+    solve's tolerance."""
+    sms, name_hash = _device_identity()
+    xn, yn, zn, sig, epsr = small_model(seed=13, dims=(37, 21, 19), nair=4)
+    src = [[("+X", 18, 10, 5)], [("+Y", 9, 12, 6)]]
+    w = [2 * np.pi * f for f in (0.3, 3.0, 30.0)]
+    kind = 1 + (2 if precision == "fused64" else 0)  # eps-bar present (model C), complex128 pass
+    out = []
+    for ts in (0, 1):
+        # the process keeps tuned choices per (mesh, batch): the second shape
+        # runs a batch of four (the three systems and a copy of the first)
+        nsys = 3 + ts
+        cache = tmp_path / ("tune%d.txt" % ts)
+        cache.write_text("37 21 19 %d %d %d %d 6 0 %d\n" % (nsys, kind, sms, name_hash, ts))
+        monkeypatch.setenv("APHID_TUNE_CACHE", str(cache))
+        with Solver(graph_iters=8) as s:
+            s.set_nodes(xn, yn, zn)
+            s.set_model("C", sig, epsr)
+            X, inf = s.sweep(w + w[:ts], src, [0, 1, 0, 0][:nsys], precision=precision, target=1e-9)
+            assert s.sweep_tile_shape() == ts and s.sweep_plane_kz() == 6
+            assert all(i["status_name"] == "converged" for i in inf), inf
+            g = O.Grid(xn, yn, zn)
+            k2 = O.gen_k2(g, O.sigma_hat("C", w[0], sig_re=sig, eps_rel=epsr), w[0])
+            rng = np.random.default_rng(7)
+            x = rng.standard_normal(g.n) + 1j * rng.standard_normal(g.n)
+            y64 = O.inprod(g, k2, x)
+            y = s.sweep_apply(x)  # system 0: w[0]
+            assert relerr(y, y64) < (1e-6 if precision == "mixed" else 1e-13)
+            out.append(X[:3])
+        assert len(cache.read_text().splitlines()) == 1  # the record was used, not retuned
+    for a, b in zip(*out):
+        assert relerr(a, b) < 1e-7
 
 
 @pytest.mark.parametrize("precision,tol_norm,tol_row", [("mixed", 1e-6, 1e-5), ("fused64", 1e-13, 1e-11)])
