@@ -4,7 +4,9 @@
 //
 // The rows are those of rows64 (inprod_x/y/z/p, src/aphid.f90:841-865,
 // 970-994, 1098-1122, 1227-1276), with the same arithmetic in the same
-// order, on the reference's [Ax|Ay|Az|Phi] layout.  What changes is where the
+// order except that the divisions by cell lengths are multiplications by
+// their reciprocals (18 FP64 divides per node were the kernel's critical
+// path), on the reference's [Ax|Ay|Az|Phi] layout.  What changes is where the
 // neighbours come from.  rows64 reads about 40 complex128 values per node
 // straight from global memory, most of them neighbours that other threads
 // also read; at 166 registers and 4 warps per block that kernel is
@@ -127,6 +129,9 @@ static __global__ void __launch_bounds__(kAThreads, 2) k_apply64s(GridDev g, Til
   const int ic = min(i, nx - 1), jc = min(j, ny - 1);
   const double xn4 = X.n4[ic], xn5 = X.n5[ic], yn4 = Y.n4[jc], yn5 = Y.n5[jc];
   const double dxc = X.dc[ic], dyc = Y.dc[jc];
+  // reciprocals of the lengths the rows divide by, once per thread (x / d
+  // becomes x (1/d): within an ulp, and no FP64 divide in the plane loop)
+  const double rdxc = 1.0 / dxc, rdyc = 1.0 / dyc, rdxi = 1.0 / X.d[ic + 1], rdyj = 1.0 / Y.d[jc + 1];
   const bool hx = live && i < nx - 1, hy = live && j < ny - 1;
   const bool pxy = live && i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
 
@@ -157,7 +162,7 @@ static __global__ void __launch_bounds__(kAThreads, 2) k_apply64s(GridDev g, Til
     auto cur = [&](int a, int off) { return C[a * kAN + me + off]; };
     auto nxt = [&](int a) { return Nx[a * kAN + me]; };
     const double2 phc = cur(SA_PH, 0), kpc = cur(SK_PH, 0);
-    const double zn4 = Z.n4[k], zn5 = Z.n5[k], dzc = Z.dc[k];
+    const double zn4 = Z.n4[k], zn5 = Z.n5[k], dzc = Z.dc[k], rdzc = 1.0 / dzc, rdzk = 1.0 / Z.d[k + 1];
     double2 e = make_double2(0.0, 0.0);
     if (live) {
       const long long pc = ixp(g, i, j, k);
@@ -179,9 +184,9 @@ static __global__ void __launch_bounds__(kAThreads, 2) k_apply64s(GridDev g, Til
         t = cadd(t, cmul(c6, nxt(SA_PH)));
         t = cadd(t, cmul(c7, phm));
         const double2 acc = rmul(vol, t);
-        const double2 d2 = rdiv(csub(s2, s1), dxc), d3 = cneg(rdiv(csub(s3, s1), dxc));
-        const double2 d4 = rdiv(csub(s4, s1), dyc), d5 = cneg(rdiv(csub(s5, s1), dyc));
-        const double2 d6 = rdiv(csub(s6, s1), dzc), d7 = cneg(rdiv(csub(s7, s1), dzc));
+        const double2 d2 = rmul(rdxc, csub(s2, s1)), d3 = cneg(rmul(rdxc, csub(s3, s1)));
+        const double2 d4 = rmul(rdyc, csub(s4, s1)), d5 = cneg(rmul(rdyc, csub(s5, s1)));
+        const double2 d6 = rmul(rdzc, csub(s6, s1)), d7 = cneg(rmul(rdzc, csub(s7, s1)));
         double2 u = cmul(d2, cur(SA_AX, 0));
         u = cadd(u, cmul(d3, cur(SA_AX, -1)));
         u = cadd(u, cmul(d4, cur(SA_AY, 0)));
@@ -205,7 +210,7 @@ static __global__ void __launch_bounds__(kAThreads, 2) k_apply64s(GridDev g, Til
         t = cadd(t, rmul(yn5, cur(SA_AX, -kAW)));
         t = cadd(t, rmul(zn4, nxt(SA_AX)));
         t = cadd(t, rmul(zn5, axm));
-        const double2 gr = rdiv(csub(cmul(cur(SA_PH, 1), csub(kp2, kx)), cmul(phc, csub(kpc, kx))), dxi);
+        const double2 gr = rmul(rdxi, csub(cmul(cur(SA_PH, 1), csub(kp2, kx)), cmul(phc, csub(kpc, kx))));
         const double2 ox = rmul(vol, cadd(t, gr));
         out[ixx(g, i, j, k)] = ox;
         e = cadd(e, cmul(axc, ox));
@@ -223,7 +228,7 @@ static __global__ void __launch_bounds__(kAThreads, 2) k_apply64s(GridDev g, Til
         t = cadd(t, rmul(xn5, cur(SA_AY, -1)));
         t = cadd(t, rmul(zn4, nxt(SA_AY)));
         t = cadd(t, rmul(zn5, aym));
-        const double2 gr = rdiv(csub(cmul(cur(SA_PH, kAW), csub(kp2, ky)), cmul(phc, csub(kpc, ky))), dyj);
+        const double2 gr = rmul(rdyj, csub(cmul(cur(SA_PH, kAW), csub(kp2, ky)), cmul(phc, csub(kpc, ky))));
         const double2 oy = rmul(vol, cadd(t, gr));
         out[ixy(g, i, j, k)] = oy;
         e = cadd(e, cmul(ayc, oy));
@@ -241,7 +246,7 @@ static __global__ void __launch_bounds__(kAThreads, 2) k_apply64s(GridDev g, Til
         t = cadd(t, rmul(xn5, cur(SA_AZ, -1)));
         t = cadd(t, rmul(yn4, cur(SA_AZ, kAW)));
         t = cadd(t, rmul(yn5, cur(SA_AZ, -kAW)));
-        const double2 gr = rdiv(csub(cmul(nxt(SA_PH), csub(kp2, kz)), cmul(phc, csub(kpc, kz))), dzk);
+        const double2 gr = rmul(rdzk, csub(cmul(nxt(SA_PH), csub(kp2, kz)), cmul(phc, csub(kpc, kz))));
         const double2 oz = rmul(vol, cadd(t, gr));
         out[ixz(g, i, j, k)] = oz;
         e = cadd(e, cmul(azc, oz));

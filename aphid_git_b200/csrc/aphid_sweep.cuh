@@ -1304,10 +1304,20 @@ __device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, 
     }
   };
 
-  // per-thread axis coefficients
+  // axis coefficients of the tile's columns and rows, staged in shared
+  // memory and read where used (not held in registers through the plane
+  // loop: the two-blocks-per-SM configuration has 128 registers per thread)
   const int ic = min(i, nx - 1), jc = min(j, ny - 1);
   const float4 *AX = D.ax32, *AY = D.ax32 + 2 * nx, *AZ = D.ax32 + 2 * (nx + ny);
-  const float4 XA = __ldg(AX + ic), XB = __ldg(AX + nx + ic), YA = __ldg(AY + jc), YB = __ldg(AY + ny + jc);
+  __shared__ float4 s_axis[2 * PT<1>::I + 2 * PT<0>::J];  // XA XB per column, YA YB per row
+  if (ty == 0) {
+    s_axis[tx] = __ldg(AX + ic);
+    s_axis[kPTI + tx] = __ldg(AX + nx + ic);
+  }
+  if (tx == 0) {
+    s_axis[2 * kPTI + ty] = __ldg(AY + jc);
+    s_axis[2 * kPTI + kPTJ + ty] = __ldg(AY + ny + jc);
+  }
   const bool hx = live && i < nx - 1, hy = live && j < ny - 1;
   const bool pxy = live && i > 0 && i < nx - 1 && j > 0 && j < ny - 1;
 
@@ -1359,6 +1369,7 @@ __device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, 
     const float sx = rk[ck], sy = rk[kKN + ck], sz = rk[2 * kKN + ck], sp0 = rk[3 * kKN + ck];
     const float ex = EPS ? re[ck] : 1.f, ey = EPS ? re[kKN + ck] : 1.f;
     const float ez = EPS ? re[2 * kKN + ck] : 1.f, ep0 = EPS ? re[3 * kKN + ck] : 1.f;
+    const float4 XA = s_axis[tx], XB = s_axis[kPTI + tx], YA = s_axis[2 * kPTI + ty], YB = s_axis[2 * kPTI + kPTJ + ty];
     if (live) {
       const float xn4 = XA.x, xn5 = XA.y, dxc = XA.z, rdxc = XA.w, ce2x = XB.x, ce3x = XB.y, dxi = XB.z,
                   rdxi = XB.w;
@@ -1491,14 +1502,6 @@ __device__ __forceinline__ bool pass_block_init(unsigned char *shm, unsigned lon
   }
   return aligned;
 }
-// the plane tiles of D are of shape TS (the launch picked the instance from
-// them); otherwise the block takes no work and the launch reports the error
-template <int TS>
-__device__ __forceinline__ bool tiles_are(const SweepDev &D, int *err) {
-  if (D.tp.ts == TS) return true;
-  if (threadIdx.x == 0) atomicExch(err, 3);
-  return false;
-}
 // the last block out of a persistent launch re-arms its work counter
 __device__ __forceinline__ void pass_block_done(int *work) {
   if (threadIdx.x == 0) {
@@ -1518,7 +1521,9 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG, TS>::blocks) k_sw
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * SH::ubytes);
-  const bool aligned = pass_block_init<SH::stages>(shm, bar, D.err) && tiles_are<TS>(D, D.err);
+  // the host launches the instance of D.tp.ts (launch_pass); no device check:
+  // a test here pushed the two-blocks-per-SM instance into spilling registers
+  const bool aligned = pass_block_init<SH::stages>(shm, bar, D.err);
   unsigned phase = 0;  // bit q: parity of the next wait on stage q
   const long long total = aligned ? D.tp.count() * D.nsys : 0;
   for (;;) {
@@ -1552,8 +1557,7 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG, TS>::blocks) k_sw
   extern __shared__ __align__(128) unsigned char shm[];
   __shared__ int s_item;
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * SH::ubytes);
-  bool aligned = pass_block_init<SH::stages>(shm, bar, G.D[0].err);
-  for (int m = 0; m < G.n; m++) aligned = aligned && tiles_are<TS>(G.D[m], G.D[0].err);
+  const bool aligned = pass_block_init<SH::stages>(shm, bar, G.D[0].err);  // all meshes in tile shape TS (run_group)
   unsigned phase = 0;
   const long long total = aligned ? G.first[G.n] : 0;
   for (;;) {
@@ -1664,9 +1668,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
   __shared__ int s_item;
   double2 *Ub = reinterpret_cast<double2 *>(shm + kStages64 * kStage);  // [2][4][kPN]
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + kStages64 * kStage + 2 * Pass64Shm<TS>::ubytes);
-  bool aligned = (smem_u32(shm) & 127u) == 0;
+  const bool aligned = (smem_u32(shm) & 127u) == 0;  // tile shape TS: launch_pass64
   if (!aligned && threadIdx.x == 0) atomicExch(D.err, 2);
-  aligned = aligned && tiles_are<TS>(D, D.err);
   if (threadIdx.x == 0 && aligned) {
 #pragma unroll
     for (int q = 0; q < kStages64; q++) mbar_init(smem_u32(&bar[q]));
