@@ -834,6 +834,7 @@ SweepDev sweep_dev(aphid_ctx *ctx, int nsys) {
   D.tmix = 1.f;
   D.work = ctx->sw_work;
   D.order = ctx->sw_work ? ctx->sw_work + 2 : nullptr;
+  D.active = ctx->sw_cnt ? reinterpret_cast<int *>(ctx->sw_cnt + (size_t)CNT_KINDS * ctx->sw_nsys) : nullptr;
   const size_t vec = (size_t)ctx->sw_nsys * ctx->n;
   const size_t v32 = (size_t)ctx->sw_nsys * 4 * ctx->nl.N;
   if (ctx->sw_f32_ok) {
@@ -970,7 +971,8 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     if (rc) return rc;
     CK(cudaMalloc(&ctx->sw_sys, (size_t)nsys * sizeof(SweepSys)));
     CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * kParts * sizeof(double)));
-    CK(cudaMalloc(&ctx->sw_cnt, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
+    // the counters, then the active-system list of the fused passes (k_sw_active)
+    CK(cudaMalloc(&ctx->sw_cnt, ((size_t)CNT_KINDS * nsys + 1 + nsys) * sizeof(unsigned)));
     CK(cudaMemset(ctx->sw_cnt, 0, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
     if (!ctx->sw_ndone) CK(cudaMalloc(&ctx->sw_ndone, sizeof(int)));
     ctx->sw_nsys = nsys;
@@ -1179,12 +1181,13 @@ void launch_pass64(aphid_ctx *ctx, const SweepDev &D0, bool timing) {
 // after every R of them, and the true-residual monitor.
 template <typename T>
 void sweep_round_t(aphid_ctx *ctx, const SweepDev &D) {
-  const unsigned ps = (unsigned)(D.bps * D.nsys);
+  const unsigned ps = (unsigned)(4 * ctx->num_sms);  // k_sw_dxupd: every block serves every pending system
   const unsigned st = (unsigned)(D.t.count() * D.nsys);
   const int ring = sizeof(T) == sizeof(double2) ? D.ring64 : D.ring;
   k_sw_dxupd<T, false><<<ps, kStreamThreads, 0, ctx->stream>>>(D);
   k_sw_resid<T><<<st, kOpThreads, 0, ctx->stream>>>(D);
   for (int it = 0; it < ctx->graph_iters; it++) {
+    k_sw_active<<<1, 1024, 0, ctx->stream>>>(D);  // the systems this pass serves
     if (sizeof(T) == sizeof(double2))
       launch_pass64(ctx, D, false);
     else
@@ -1295,7 +1298,9 @@ void device_identity(const aphid_ctx *ctx, int &sms, int &name_hash) {
 // The complex64 pass is timed for every (ts, cfg, kz): the two tile shapes of
 // PT, the two pipeline configurations of PassShm (two stages with two blocks
 // per SM for model R, or three stages in one) and the z-slab depths; the
-// complex128 pass for (ts, kz).
+// complex128 pass for (ts, kz).  The timing uses events of its own: a sweep
+// that tunes in the middle (AUTO's escalation phase) keeps its own start
+// event.
 int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
   int sms, name_hash;
   device_identity(ctx, sms, name_hash);
@@ -1313,6 +1318,16 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
     if (rc0) return rc0;
     CK(cudaMemsetAsync(ctx->sw_sys, 0, (size_t)nsys * sizeof(SweepSys), ctx->stream));
     CK(cudaMemsetAsync(ctx->sw_err, 0, sizeof(int), ctx->stream));
+    struct TuneEvents {  // released on every return
+      cudaEvent_t e[2] = {nullptr, nullptr};
+      ~TuneEvents() {
+        for (cudaEvent_t x : e)
+          if (x) cudaEventDestroy(x);
+      }
+    } own;
+    CK(cudaEventCreate(&own.e[0]));
+    CK(cudaEventCreate(&own.e[1]));
+    cudaEvent_t *tev = own.e;
     float best_ms = 0.f;
     const int cand[] = {4, 6, 8, 12, 16, 24, 32};
     for (int ts = 0; ts < kTileShapes; ts++)
@@ -1334,13 +1349,13 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
             launch_pass(ctx, D, true);
         };
         for (int r = 0; r < 2; r++) pass();
-        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        CK(cudaEventRecord(tev[0], ctx->stream));
         for (int r = 0; r < 5; r++) pass();
-        CK(cudaEventRecord(ctx->ev1, ctx->stream));
-        CK(cudaEventSynchronize(ctx->ev1));
+        CK(cudaEventRecord(tev[1], ctx->stream));
+        CK(cudaEventSynchronize(tev[1]));
         CK(cudaGetLastError());
         float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        CK(cudaEventElapsedTime(&ms, tev[0], tev[1]));
         if (!best.kz || ms < best_ms) {
           best = Tuned{c, cfg, ts};
           best_ms = ms;
@@ -1419,7 +1434,7 @@ int run_batched(aphid_ctx *ctx, const SweepDev &D, bool fused, std::vector<Sweep
   CK(cudaGetLastError());
   nlaunch += 1;
   if ((rc = sweep_graph(ctx, D, fused))) return rc;
-  const long long per_round = 3 + (long long)ctx->graph_iters + ctx->graph_iters / (fused ? D.ring64 : D.ring);
+  const long long per_round = 3 + 2LL * ctx->graph_iters + ctx->graph_iters / (fused ? D.ring64 : D.ring);
   const long long max_rounds = (long long)std::max(1, max_it) / ctx->graph_iters + 2LL * (hs[0].max_outer + 2);
   for (long long round = 0;; round++) {
     CK(cudaMemcpyAsync(ctx->h_ndone, ctx->sw_ndone, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1858,6 +1873,13 @@ int sweep_finish(aphid_ctx *ctx, SweepPrep &P, const double *omega, const aphid_
     std::vector<int> esc;
     for (int s = 0; s < P.nsys; s++)
       if (P.hs[s].status == kStEscalated) esc.push_back(s);
+    if (ctx->verbose && own_events && !esc.empty()) {
+      float m1 = 0.f;
+      CK(cudaEventRecord(ctx->ev1, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      CK(cudaEventElapsedTime(&m1, ctx->ev0, ctx->ev1));
+      std::fprintf(stderr, "aphid_gpu: complex64 phase %.3f s, %zu systems escalated\n", m1 * 1e-3, esc.size());
+    }
     if (!esc.empty() && (rc = finish_escalated(ctx, omega, opts, esc, P.out, P.nlaunch))) return rc;
   }
   float ms = 0.f;

@@ -79,6 +79,12 @@ constexpr double kStagnation = 16.0;
 // reached.  Complex128 inner solves track the true residual, so their monitor
 // waits for 10 x the target (SweepSys::mon_level).
 constexpr double kMonitorLevel = 1e-4;
+// Between that level and kCheckNear x the target the monitor checks every
+// kCheckEvery inner iterations instead of every graph round: each check is a
+// complex128 operator over the system, about a sixth of a round's cost when a
+// system runs on alone for thousands of iterations.
+constexpr double kCheckNear = 10.0;
+constexpr int kCheckEvery = 64;
 // rho_{n+1}^2 from the expansion ||q||^2 - 2 Re(conj(beta) v^H q) + |beta|^2
 // ||v||^2 is trusted down to this fraction of ||q||^2; below it the new
 // Lanczos vector is treated as zero (the iterate is final for this cycle).
@@ -128,6 +134,7 @@ struct SweepSys {
   double ratio_min, mon_rn;  // true-residual monitor of the running inner cycle
   int phase, has_inner, inner_it, total_it, outer_it, max_it, max_outer, status;
   int checks;
+  int last_check_it;         // total_it at the monitor's last check
   int cur;                   // buffer set holding q^, v^ of the last pass
   int restarts;              // inner cycles ended by kCancel / kDrift / a stall
   double tau_win;            // tau at the start of the current stall window
@@ -191,6 +198,7 @@ struct SweepDev {
   int timing;                    // fused passes: 1 in timing launches (see k_sw_pass)
   int *work;                     // [2]: next work item, blocks finished (complex64 pass)
   const int *order;              // plane tiles in the order the pass takes them
+  int *active;                   // [1 + nsys]: count, then the systems in their inner cycle (k_sw_active)
   // complex128 inner storage (k_sw_pass64): same layouts, double2
   double2 *W64, *P64, *dd64;
   int ring64;
@@ -289,35 +297,58 @@ __device__ __forceinline__ void jacobi_weights(float2 z, float2 &inv, float &abs
 // The same two functions in FP64 for the complex128 pass (k_sw_pass64) and
 // the kernels that share its state: the diagonal of K from the FP64 axis
 // tables and sigma-bar, and D^-1, |D|, 1/|D| -- all with non-contracting
-// intrinsics so that every kernel forms bit-identical values.
+// intrinsics so that every kernel forms bit-identical values.  jacobi64 is
+// assembled from its pieces: the entry of one edge component (vol, the sum of
+// the row's coefficients, sigma-bar and eps-bar of the edge) and of an
+// interior Phi node, so that a kernel forming only some components of a node
+// gets the bits that jacobi64 gives.
+__device__ __forceinline__ double2 jac64_edge(double vol, double sum, double s_, double e_, double ka, double kb) {
+  return make_double2(__dmul_rn(vol, __dsub_rn(-__dmul_rn(ka, e_), sum)), __dmul_rn(vol, __dmul_rn(kb, s_)));
+}
+__device__ __forceinline__ double2 jac64_x(double4 XA, double4 XB, double4 YA, double4 ZA, double sx, double ex,
+                                           double ka, double kb) {
+  auto M = [](double a, double b) { return __dmul_rn(a, b); };
+  auto A = [](double a, double b) { return __dadd_rn(a, b); };
+  return jac64_edge(M(M(XB.z, YA.z), ZA.z), A(A(A(A(A(XB.x, XB.y), YA.x), YA.y), ZA.x), ZA.y), sx, ex, ka, kb);
+}
+__device__ __forceinline__ double2 jac64_y(double4 XA, double4 YA, double4 YB, double4 ZA, double sy, double ey,
+                                           double ka, double kb) {
+  auto M = [](double a, double b) { return __dmul_rn(a, b); };
+  auto A = [](double a, double b) { return __dadd_rn(a, b); };
+  return jac64_edge(M(M(XA.z, YB.z), ZA.z), A(A(A(A(A(YB.x, YB.y), XA.x), XA.y), ZA.x), ZA.y), sy, ey, ka, kb);
+}
+__device__ __forceinline__ double2 jac64_z(double4 XA, double4 YA, double4 ZA, double4 ZB, double sz, double ez,
+                                           double ka, double kb) {
+  auto M = [](double a, double b) { return __dmul_rn(a, b); };
+  auto A = [](double a, double b) { return __dadd_rn(a, b); };
+  return jac64_edge(M(M(XA.z, YA.z), ZB.z), A(A(A(A(A(ZB.x, ZB.y), XA.x), XA.y), YA.x), YA.y), sz, ez, ka, kb);
+}
+__device__ __forceinline__ double2 jac64_p(double4 XA, double4 YA, double4 ZA, double sx, double sy, double sz,
+                                           double sp0, double sxm, double sym, double s2m, double ex, double ey,
+                                           double ez, double ep0, double exm, double eym, double e2m, double ka,
+                                           double kb) {
+  auto M = [](double a, double b) { return __dmul_rn(a, b); };
+  auto A = [](double a, double b) { return __dadd_rn(a, b); };
+  const double xn4 = XA.x, xn5 = XA.y, dxc = XA.z, yn4 = YA.x, yn5 = YA.y, dyc = YA.z, zn4 = ZA.x, zn5 = ZA.y,
+               dzc = ZA.z;
+  const double vol = M(M(dxc, dyc), dzc);
+  const double s1r = -M(ka, ep0), s1i = M(kb, sp0);
+  const double nr = A(A(A(A(A(M(xn4, ex), M(xn5, exm)), M(yn4, ey)), M(yn5, eym)), M(zn4, ez)), M(zn5, e2m));
+  const double ni = A(A(A(A(A(M(xn4, sx), M(xn5, sxm)), M(yn4, sy)), M(yn5, sym)), M(zn4, sz)), M(zn5, s2m));
+  const double pr = __dsub_rn(M(s1r, s1r), M(s1i, s1i)), pi = M(2.0, M(s1r, s1i));
+  return make_double2(M(vol, A(pr, M(ka, nr))), M(vol, __dsub_rn(pi, M(kb, ni))));
+}
 __device__ __forceinline__ void jacobi64(double4 XA, double4 XB, double4 YA, double4 YB, double4 ZA, double4 ZB,
                                          double sx, double sy, double sz, double sp0, double sxm, double sym,
                                          double s2m, double ex, double ey, double ez, double ep0, double exm,
                                          double eym, double e2m, bool hx, bool hy, bool hz, bool pin, double ka,
                                          double kb, double2 dg[4]) {
-  auto M = [](double a, double b) { return __dmul_rn(a, b); };
-  auto A = [](double a, double b) { return __dadd_rn(a, b); };
-  auto edge = [&](double vol, double sum, double s_, double e_) {
-    return make_double2(M(vol, __dsub_rn(-M(ka, e_), sum)), M(vol, M(kb, s_)));
-  };
-  const double xn4 = XA.x, xn5 = XA.y, dxc = XA.z, yn4 = YA.x, yn5 = YA.y, dyc = YA.z, zn4 = ZA.x, zn5 = ZA.y,
-               dzc = ZA.z;
-  dg[0] = hx ? edge(M(M(XB.z, dyc), dzc), A(A(A(A(A(XB.x, XB.y), yn4), yn5), zn4), zn5), sx, ex)
-             : make_double2(0.0, 0.0);
-  dg[1] = hy ? edge(M(M(dxc, YB.z), dzc), A(A(A(A(A(YB.x, YB.y), xn4), xn5), zn4), zn5), sy, ey)
-             : make_double2(0.0, 0.0);
-  dg[2] = hz ? edge(M(M(dxc, dyc), ZB.z), A(A(A(A(A(ZB.x, ZB.y), xn4), xn5), yn4), yn5), sz, ez)
-             : make_double2(0.0, 0.0);
-  if (pin) {
-    const double vol = M(M(dxc, dyc), dzc);
-    const double s1r = -M(ka, ep0), s1i = M(kb, sp0);
-    const double nr = A(A(A(A(A(M(xn4, ex), M(xn5, exm)), M(yn4, ey)), M(yn5, eym)), M(zn4, ez)), M(zn5, e2m));
-    const double ni = A(A(A(A(A(M(xn4, sx), M(xn5, sxm)), M(yn4, sy)), M(yn5, sym)), M(zn4, sz)), M(zn5, s2m));
-    const double pr = __dsub_rn(M(s1r, s1r), M(s1i, s1i)), pi = M(2.0, M(s1r, s1i));
-    dg[3] = make_double2(M(vol, A(pr, M(ka, nr))), M(vol, __dsub_rn(pi, M(kb, ni))));
-  } else {
-    dg[3] = make_double2(1.0, 0.0);
-  }
+  const double2 zero = make_double2(0.0, 0.0);
+  dg[0] = hx ? jac64_x(XA, XB, YA, ZA, sx, ex, ka, kb) : zero;
+  dg[1] = hy ? jac64_y(XA, YA, YB, ZA, sy, ey, ka, kb) : zero;
+  dg[2] = hz ? jac64_z(XA, YA, ZA, ZB, sz, ez, ka, kb) : zero;
+  dg[3] = pin ? jac64_p(XA, YA, ZA, sx, sy, sz, sp0, sxm, sym, s2m, ex, ey, ez, ep0, exm, eym, e2m, ka, kb)
+              : make_double2(1.0, 0.0);
 }
 __device__ __forceinline__ void jacobi_weights(double2 z, double2 &inv, double &absd, double &rabsd) {
   // |z|^2 stays far inside the FP64 range here, so no pre-scaling: one
@@ -739,72 +770,79 @@ __device__ __forceinline__ float2 dx_link(float2 e, float2 p, float k, float2 d)
 __device__ __forceinline__ double2 dx_link(double2 e, double2 p, double k, double2 d) {
   return make_double2(fma(e.x, p.x, fma(-e.y, p.y, k * d.x)), fma(e.x, p.y, fma(e.y, p.x, k * d.y)));
 }
+// Every block takes a slice of every system with pending updates (blocks
+// stride over the nodes of one system, then go on to the next system), so
+// that when only a few systems are still running their updates are spread
+// over the whole grid rather than over a fixed per-system share of it.
 template <typename T, bool TIMING>
 static __global__ void __launch_bounds__(kStreamThreads) k_sw_dxupd(SweepDev D) {
-  const int sys = blockIdx.x % D.nsys, chunk = blockIdx.x / D.nsys;
-  SweepSys *S = D.sys + sys;
   using R = typename Inner<T>::R;
   const int ring = Inner<T>::ring(D);
   __shared__ int s_np;
   __shared__ T s_eta[kMaxRing];
   __shared__ R s_kap[kMaxRing];
   __shared__ const T *s_p[kMaxRing];
-  if (threadIdx.x == 0) s_np = TIMING ? ring : S->npend;
-  __syncthreads();
-  const int np = s_np;
-  if (np == 0) return;
-  if (threadIdx.x < np) {
-    const int q = threadIdx.x;
-    s_eta[q] = TIMING ? Inner<T>::from_d(make_double2(0.0, 0.0)) : Inner<T>::from_d(S->eta_h[q]);
-    s_kap[q] = TIMING ? (R)1 : (R)S->kap_h[q];
-    s_p[q] = Inner<T>::pv(D, TIMING ? (S->pslot + 1 + q) % (ring + 1) : S->slot_h[q], sys);
-  }
-  __syncthreads();
   const double mix = TIMING ? (double)D.tmix : 1.0;
-  T *dd = Inner<T>::dd(D) + (long long)sys * 4 * D.L.N;
   const GridDev &g = D.g;
-  const long long plane = (long long)D.L.nxp * g.ny;
-  double2 *x64 = D.x64 + (long long)sys * D.n;
-  for (long long nd = chunk * (long long)blockDim.x + threadIdx.x; nd < D.L.N;
-       nd += (long long)D.bps * blockDim.x) {
-    const int k = (int)(nd / plane);
-    const long long r = nd - k * plane;
-    const int j = (int)(r / D.L.nxp), i = (int)(r - (long long)j * D.L.nxp);
-    if (i >= g.nx) continue;
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      if (!exists(g, c, i, j, k)) continue;
-      const long long t = c * D.L.N + nd;
-      const long long rt = ref_of(g, c, i, j, k);
-      // every load of this unknown first (the ring slots, d^, x), then the
-      // recurrence: the loads are in flight together instead of one memory
-      // latency per pending update
-      T pj[kMaxRing];
-#pragma unroll
-      for (int q = 0; q < kMaxRing; q++)
-        if (q < np) pj[q] = __ldg(s_p[q] + t);
-      T d = dd[t];
-      const double2 x0 = x64[rt];
-      double2 dx = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int q = 0; q < kMaxRing; q++)
-        if (q < np) {
-          d = dx_link(s_eta[q], pj[q], s_kap[q], d);
-          dx = cadd(dx, to_d(d));
-        }
-      dd[t] = d;
-      x64[rt] = make_double2(fma(mix, dx.x, x0.x), fma(mix, dx.y, x0.y));
+  // node indices in 32 bits (the sweep limits a system to 2^31 node-layout
+  // values): two 32-bit divisions per node instead of two 64-bit ones
+  const unsigned nxp = (unsigned)D.L.nxp, ny = (unsigned)g.ny, nn = (unsigned)D.L.N;
+  for (int sys = 0; sys < D.nsys; sys++) {
+    SweepSys *S = D.sys + sys;
+    __syncthreads();  // the previous system's list is no longer read
+    if (threadIdx.x == 0) s_np = TIMING ? ring : S->npend;
+    __syncthreads();
+    const int np = s_np;
+    if (np == 0) continue;
+    if (threadIdx.x < np) {
+      const int q = threadIdx.x;
+      s_eta[q] = TIMING ? Inner<T>::from_d(make_double2(0.0, 0.0)) : Inner<T>::from_d(S->eta_h[q]);
+      s_kap[q] = TIMING ? (R)1 : (R)S->kap_h[q];
+      s_p[q] = Inner<T>::pv(D, TIMING ? (S->pslot + 1 + q) % (ring + 1) : S->slot_h[q], sys);
     }
-  }
-  // the last block of this system empties its pending list
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned *cnt = D.cnt + CNT_DX * D.nsys + sys;
-    if (atomicAdd(cnt, 1u) == (unsigned)D.bps - 1) {
-      if (!TIMING) S->npend = 0;
-      *cnt = 0;
+    __syncthreads();
+    T *dd = Inner<T>::dd(D) + (long long)sys * 4 * D.L.N;
+    double2 *x64 = D.x64 + (long long)sys * D.n;
+    for (unsigned nd = blockIdx.x * blockDim.x + threadIdx.x; nd < nn; nd += gridDim.x * blockDim.x) {
+      const unsigned row = nd / nxp, iu = nd - row * nxp;
+      if (iu >= (unsigned)g.nx) continue;
+      const unsigned ku = row / ny;
+      const int i = (int)iu, j = (int)(row - ku * ny), k = (int)ku;
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        if (!exists(g, c, i, j, k)) continue;
+        const long long t = c * D.L.N + nd;
+        const long long rt = ref_of(g, c, i, j, k);
+        // every load of this unknown first (the ring slots, d^, x), then the
+        // recurrence: the loads are in flight together instead of one memory
+        // latency per pending update
+        T pj[kMaxRing];
+#pragma unroll
+        for (int q = 0; q < kMaxRing; q++)
+          if (q < np) pj[q] = __ldg(s_p[q] + t);
+        T d = dd[t];
+        const double2 x0 = x64[rt];
+        double2 dx = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < kMaxRing; q++)
+          if (q < np) {
+            d = dx_link(s_eta[q], pj[q], s_kap[q], d);
+            dx = cadd(dx, to_d(d));
+          }
+        dd[t] = d;
+        x64[rt] = make_double2(fma(mix, dx.x, x0.x), fma(mix, dx.y, x0.y));
+      }
+    }
+    // the last block through this system empties its pending list
+    __syncthreads();
+    if (threadIdx.x == 0) {
       __threadfence();
+      unsigned *cnt = D.cnt + CNT_DX * D.nsys + sys;
+      if (atomicAdd(cnt, 1u) == gridDim.x - 1) {
+        if (!TIMING) S->npend = 0;
+        *cnt = 0;
+        __threadfence();
+      }
     }
   }
 }
@@ -920,7 +958,12 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
   const long long tile = blockIdx.x / D.nsys;
   SweepSys *S = D.sys + sys;
   if (S->phase != PH_INNER || S->inner_it < 2) return;
-  if (S->rnorm * (S->tau / S->tau0) > S->mon_level * S->bnorm) return;
+  const double pred = S->rnorm * (S->tau / S->tau0);  // the true residual the quasi-residual predicts
+  if (pred > S->mon_level * S->bnorm) return;
+  // near the target every round (the check ends the cycle on convergence);
+  // further away every kCheckEvery iterations (it ends the cycle when the
+  // true residual stops following the quasi-residual)
+  if (pred > kCheckNear * S->target * S->bnorm && S->total_it - S->last_check_it < kCheckEvery) return;
   int i, j, k0, k1;
   sweep_tile(D, tile, i, j, k0, k1);
   Vals<1> a{{0.0}};
@@ -946,6 +989,7 @@ static __global__ void __launch_bounds__(kOpThreads) k_sw_check(SweepDev D) {
       const double rn = sqrt(tot.v[0]);
       S->mon_rn = rn;
       S->checks++;
+      S->last_check_it = S->total_it;
       const double ratio = rn / fmax(S->tau, 1e-300);
       S->ratio_min = fmin(S->ratio_min, ratio);
       if (!isfinite(rn) || rn < S->target * S->bnorm || ratio > kStagnation * S->ratio_min)
@@ -1205,7 +1249,7 @@ __device__ __noinline__ void pass_scalars(SweepSys *S, const double *T, int ring
 // the mesh and buffers of D with the tensor maps M.  shm: the pass's dynamic
 // shared memory; bar, phase: its stage mbarriers and their wait parities.
 template <bool EPS, int CFG, int TS>
-__device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, long long item,
+__device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, int sys, long long tile,
                                           unsigned char *shm, unsigned long long *bar, unsigned &phase) {
   using SH = PassShm<EPS, CFG, TS>;
   constexpr int kStages = SH::stages;
@@ -1213,8 +1257,6 @@ __device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, 
   constexpr int kPTI = PT<TS>::I, kPTJ = PT<TS>::J, kPW = PT<TS>::W, kPN = PT<TS>::N, kKW = PT<TS>::KW,
                 kKN = PT<TS>::KN;
   float2 *Ub = reinterpret_cast<float2 *>(shm + kStages * kStage);  // [2][4][kPN]
-  const int sys = (int)(item % D.nsys);
-  const long long tile = __ldg(D.order + item / D.nsys);
   SweepSys *S = D.sys + sys;
   if (!D.timing && S->phase != PH_INNER) return;
 
@@ -1487,6 +1529,59 @@ __device__ __forceinline__ void pass_item(const SweepDev &D, const PassMaps &M, 
   }
 }
 
+// The systems a fused pass serves.  A persistent pass takes (tile, system)
+// work items from a counter; items of systems that have left their inner
+// cycle cost a counter round trip, two barriers and a phase read each, which
+// on a batch whose last few systems run on alone is a large part of every
+// pass.  So before each pass k_sw_active lists the systems still in their
+// inner cycle, and the pass numbers its items over those only.  Timing
+// launches (and the several-mesh group pass) serve every system.
+static __global__ void __launch_bounds__(1024) k_sw_active(SweepDev D) {
+  __shared__ int s_warp[32], s_base;
+  if (threadIdx.x == 0) s_base = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int s0 = 0; s0 < D.nsys; s0 += blockDim.x) {
+    const int s = s0 + threadIdx.x;
+    const bool on = s < D.nsys && D.sys[s].phase == PH_INNER;
+    const unsigned b = __ballot_sync(0xffffffffu, on);
+    if (lane == 0) s_warp[w] = __popc(b);
+    __syncthreads();
+    if (threadIdx.x == 0) {  // exclusive scan over the warps, ascending systems
+      int acc = s_base;
+      for (int q = 0; q < nw; q++) {
+        const int c = s_warp[q];
+        s_warp[q] = acc;
+        acc += c;
+      }
+      s_base = acc;
+    }
+    __syncthreads();
+    if (on) D.active[1 + s_warp[w] + __popc(b & ((1u << lane) - 1u))] = s;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) D.active[0] = s_base;
+}
+struct ActiveSet {
+  const int *list;  // null: every system, in order
+  long long n;      // systems served
+  // system of work item `item` (items are tile-major, systems fastest)
+  __device__ __forceinline__ int sys(long long item, long long total) const {
+    return list ? (item < total ? list[item % n] : 0) : (int)(item % n);
+  }
+};
+__device__ __forceinline__ ActiveSet active_set(const SweepDev &D) {
+  ActiveSet A;
+  if (D.active && !D.timing) {
+    A.list = D.active + 1;
+    A.n = *(volatile const int *)D.active;
+  } else {
+    A.list = nullptr;
+    A.n = D.nsys;
+  }
+  return A;
+}
+
 // set-up of a pass block: the stage mbarriers; false when the dynamic shared
 // memory is not 128-byte aligned (TMA destinations must be; the block then
 // takes no work and the launch reports the error)
@@ -1523,16 +1618,21 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG, TS>::blocks) k_sw
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(shm + SH::stages * SH::stage + 2 * SH::ubytes);
   // the host launches the instance of D.tp.ts (launch_pass); no device check:
   // a test here pushed the two-blocks-per-SM instance into spilling registers
+  __shared__ int s_sys;
   const bool aligned = pass_block_init<SH::stages>(shm, bar, D.err);
   unsigned phase = 0;  // bit q: parity of the next wait on stage q
-  const long long total = aligned ? D.tp.count() * D.nsys : 0;
+  const ActiveSet A = active_set(D);
+  const long long total = aligned ? D.tp.count() * A.n : 0;
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) s_item = atomicAdd(D.work, 1);
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(D.work, 1);
+      s_sys = A.sys(s_item, total);
+    }
     __syncthreads();
     const long long item = s_item;
     if (item >= total) break;
-    pass_item<EPS, CFG, TS>(D, M, item, shm, bar, phase);
+    pass_item<EPS, CFG, TS>(D, M, s_sys, __ldg(D.order + item / A.n), shm, bar, phase);
   }
   pass_block_done(D.work);
 }
@@ -1568,7 +1668,9 @@ __global__ void __launch_bounds__(kPThreads, PassShm<EPS, CFG, TS>::blocks) k_sw
     if (item >= total) break;
     int m = 0;
     while (m + 1 < G.n && item >= G.first[m + 1]) m++;
-    pass_item<EPS, CFG, TS>(G.D[m], G.M[m], item - G.first[m], shm, bar, phase);
+    const long long it = item - G.first[m];
+    pass_item<EPS, CFG, TS>(G.D[m], G.M[m], (int)(it % G.D[m].nsys), __ldg(G.D[m].order + it / G.D[m].nsys), shm,
+                            bar, phase);
   }
   pass_block_done(G.work);
 }
@@ -1677,16 +1779,21 @@ __global__ void __launch_bounds__(kPThreads, 1) k_sw_pass64(SweepDev D, const __
     fence_async_smem();
   }
   unsigned phase = 0;  // bit q: parity of the next wait on stage q
-  const long long per_sys = D.tp.count(), total = aligned ? per_sys * D.nsys : 0;
+  __shared__ int s_sys;
+  const ActiveSet A = active_set(D);
+  const long long total = aligned ? D.tp.count() * A.n : 0;
 
   for (;;) {
   __syncthreads();
-  if (threadIdx.x == 0) s_item = atomicAdd(D.work, 1);
+  if (threadIdx.x == 0) {
+    s_item = atomicAdd(D.work, 1);
+    s_sys = A.sys(s_item, total);
+  }
   __syncthreads();
   const long long item = s_item;
   if (item >= total) break;
-  const int sys = (int)(item % D.nsys);
-  const long long tile = __ldg(D.order + item / D.nsys);
+  const int sys = s_sys;
+  const long long tile = __ldg(D.order + item / A.n);
   SweepSys *S = D.sys + sys;
   if (!D.timing && S->phase != PH_INNER) continue;
 

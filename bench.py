@@ -290,29 +290,62 @@ def timed(stream, dev, fn, steps, barrier, world):
     return ms, out
 
 
-def field_error(s, m, om, sos, rec, Ea, Ha, idx):
-    """relative error of E and H at the receivers of systems idx (from a
-    finished sweep: Ea, Ha) against complex128 solves of the reference's
-    recurrence to 1e-12, beside the error of that recurrence itself stopped at
-    the same 1e-8 target (a 1e-8 residual does not bound every field error:
-    at 1e5 Hz in seawater the fields 2 km from the source are rounding noise
-    of the source region's).  bound = max(1e-6, 2 x the reference's own)."""
+def field_error(s, m, om, sos, rec, Ea, Ha, Xa, idx):
+    """E and H of systems idx of a finished sweep (receiver values Ea, Ha;
+    solutions Xa[q] fetched right after it) against complex128 solves of the
+    reference's recurrence to 1e-12, beside the error of that recurrence
+    itself stopped at the same 1e-8 target.
+
+    Two measures per system: the relative error over the whole mesh (E on
+    the edges, B on the faces, from gen_fields) and at the receivers.  A
+    1e-8 residual resolves a field only down to about 1e-8 of the largest
+    one, so the receiver bound has a floor: where the receivers see a field
+    that is a fraction f of the mesh-wide one (at 1e5 Hz in seawater the
+    receivers 2 km from the source see rounding noise of the source region's
+    field), no solve to 1e-8 fixes it better than 1e-8 / f.  Bounds:
+    mesh-wide max(1e-6, 2 x the reference's own error); receivers the same
+    or 1e-8 / f, whichever is larger."""
     sub = ([om[q] for q in idx], m.sources, [sos[q] for q in idx])
+    err = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    def mesh_fields(xs, oms):
+        return [s.gen_fields(w, x) for w, x in zip(oms, xs)]  # (B, E) per system
+
+    oms = [om[q] for q in idx]
+    Fa = mesh_fields([Xa[q] for q in idx], oms)
     s.sweep(*sub, precision="fp64", target=1e-12, max_it=4 * MAX_IT, fetch=False)
     Er, Hr = s.sweep_receivers(rec)
+    Fr = mesh_fields([s.sweep_fetch(r) for r in range(len(idx))], oms)
     s.sweep(*sub, precision="fp64", target=TARGET, max_it=4 * MAX_IT, fetch=False)
     E8, H8 = s.sweep_receivers(rec)
-    err = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    e = [err(Ea[q], Er[r]) for r, q in enumerate(idx)]
-    h = [err(Ha[q], Hr[r]) for r, q in enumerate(idx)]
-    e8 = [err(E8[r], Er[r]) for r in range(len(idx))]
-    h8 = [err(H8[r], Hr[r]) for r in range(len(idx))]
-    ok = all(a <= max(1e-6, 2 * b) for a, b in zip(e + h, e8 + h8))
-    return {"E": max(e), "H": max(h), "within_bound": ok,
-            "per_system": {"freq_hz": [om[q] / (2 * np.pi) for q in idx], "E": e, "H": h,
-                           "E_reference_at_1e-8": e8, "H_reference_at_1e-8": h8},
+    F8 = mesh_fields([s.sweep_fetch(r) for r in range(len(idx))], oms)
+    out = {"freq_hz": [w / (2 * np.pi) for w in oms]}
+    ok = True
+    for key, rk, ra, rr, r8, fi in (("E", "E", Ea, Er, E8, 1), ("H", "B", Ha, Hr, H8, 0)):
+        mesh = [err(Fa[r][fi], Fr[r][fi]) for r in range(len(idx))]
+        mesh8 = [err(F8[r][fi], Fr[r][fi]) for r in range(len(idx))]
+        recv = [err(ra[q], rr[r]) for r, q in enumerate(idx)]
+        recv8 = [err(r8[r], rr[r]) for r in range(len(idx))]
+        # the receivers' share of the field: their rms against the mesh's rms
+        # (B and H differ by mu0, which cancels)
+        frac = []
+        for r in range(len(idx)):
+            scale = 1.0 if key == "E" else 4e-7 * np.pi
+            rec_rms = np.linalg.norm(rr[r]) * scale / np.sqrt(rr[r].size)
+            mesh_rms = np.linalg.norm(Fr[r][fi]) / np.sqrt(Fr[r][fi].size)
+            frac.append(float(rec_rms / max(mesh_rms, 1e-300)))
+        b_mesh = [max(1e-6, 2 * b) for b in mesh8]
+        b_recv = [max(1e-6, 2 * b, 1e-8 / max(f, 1e-300)) for b, f in zip(recv8, frac)]
+        ok = ok and all(a <= b for a, b in zip(mesh, b_mesh)) and all(a <= b for a, b in zip(recv, b_recv))
+        out[key] = {"mesh": mesh, "mesh_reference_at_1e-8": mesh8, "mesh_bound": b_mesh,
+                    "receivers": recv, "receivers_reference_at_1e-8": recv8,
+                    "receiver_field_fraction": frac, "receivers_bound": b_recv}
+    return {"E": max(out["E"]["mesh"]), "H": max(out["H"]["mesh"]),
+            "E_receivers": max(out["E"]["receivers"]), "H_receivers": max(out["H"]["receivers"]),
+            "within_bound": ok, "per_system": out,
             "reference": "complex128 Jacobi-QMR (reference recurrence) to 1e-12",
-            "bound": "max(1e-6, 2 x the reference recurrence's own error at 1e-8)",
+            "bound": "mesh-wide: max(1e-6, 2 x the reference recurrence's own error at 1e-8); receivers: "
+                     "the same or 1e-8 / (receiver rms field / mesh rms field), whichever is larger",
             "receivers": int(len(rec))}
 
 
@@ -337,6 +370,10 @@ def main():
                     help="run one sweep of the workload and exit (profiling target)")
     ap.add_argument("--only-apply", action="store_true",
                     help="set up the workload and time only the fused pass (profiling)")
+    ap.add_argument("--freqs", default="",
+                    help="comma-separated frequencies (Hz) in place of the workload's own (profiling batches)")
+    ap.add_argument("--verbose", action="store_true",
+                    help="the library reports its tuning and sweep phases on stderr")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -365,7 +402,9 @@ def main():
             dist.barrier()
 
     m = model.make_model(args.workload)
-    s = Solver(device=local, stream=stream.cuda_stream)
+    if args.freqs:
+        m.freqs = np.array([float(f) for f in args.freqs.split(",")])
+    s = Solver(device=local, stream=stream.cuda_stream, verbose=args.verbose)
     s.set_nodes(m.xn, m.yn, m.zn)
     n = s.n
     om, sos = systems_of(m)
@@ -419,6 +458,10 @@ def main():
     launches = int(sum(i[0]["kernel_launches"] for i in infs if i))
     value = args.steps / (ms * 1e-3)
     Ea, Ha = s.sweep_receivers(rec) if mine else (None, None)
+    # the solutions of the field check's systems (lowest, middle, highest
+    # frequency of this rank), before the comparison legs overwrite them
+    idx_f = sorted({0, len(mine) // 2, len(mine) - 1}) if mine else []
+    Xa = {q: s.sweep_fetch(q) for q in idx_f} if not args.no_field_err else {}
 
     # ---- e2e: host buffers, copies inside the timed region
     sig_host = torch.empty(m.sig_re.shape[::-1], dtype=torch.float32, pin_memory=True).numpy().T
@@ -502,8 +545,7 @@ def main():
             extra["fused64_sweep"] = {"error": str(e)}
     if not args.no_field_err and mine:
         try:
-            idx = sorted({0, len(mine) // 2, len(mine) - 1})
-            extra["field_err"] = field_error(s, m, my_om, my_sos, rec, Ea, Ha, idx)
+            extra["field_err"] = field_error(s, m, my_om, my_sos, rec, Ea, Ha, Xa, idx_f)
         except Exception as e:
             extra["field_err"] = {"error": str(e)}
     # effective bandwidth of the inner iterations over a whole sweep (all
