@@ -25,17 +25,53 @@ int set_err(int code, const std::string &msg) {
   return code;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// a row-major BF16 matrix (rows x cols, leading dimension ld elements) as a
+// 2-D tensor of box cols_box x rows_box, 128-byte swizzle
+int bf16_map(CUtensorMap *m, const __nv_bfloat16 *base, int rows, int cols, int ld, int rows_box) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess || !f)
+      return set_err(APHID_UNET_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = (EncodeTiledFn)f;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)rows_box}, es[2] = {1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(base), dims, strides, box,
+                        es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_err(APHID_UNET_ERR_CUDA, "cuTensorMapEncodeTiled (gemm): " + std::to_string((int)r));
+  return APHID_UNET_OK;
+}
+
 template <int BN, int OUT>
 int launch_gemm_t(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int ldb, void *C, int ldc,
                   const float *bias, int M, int N, int K, int splitk, cudaStream_t st, int *err) {
-  const size_t shm = GemmShm<BN>::bytes;
-  if (cudaFuncSetAttribute(k_gemm_bf16<BN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) !=
-      cudaSuccess)
-    return set_err(APHID_UNET_ERR_CUDA, "cudaFuncSetAttribute (gemm)");
+  const size_t shm = TmaShm<BN>::bytes;
+  static bool attr = false;  // once per instantiation and process
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_gemm_tma<BN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) !=
+        cudaSuccess)
+      return set_err(APHID_UNET_ERR_CUDA, "cudaFuncSetAttribute (gemm)");
+    attr = true;
+  }
+  CUtensorMap ma, mb;
+  int rc;
+  if ((rc = bf16_map(&ma, A, M, K, lda, kBM)) || (rc = bf16_map(&mb, B, N, K, ldb, BN))) return rc;
   const int nkb = K / kBK;
   const int per = (nkb + splitk - 1) / splitk;
+  // 16-byte output stores where every row start is 16-byte aligned
+  const size_t es = (OUT == OUT_BF16_RELU || OUT == OUT_BF16) ? 2 : 4;
+  const int vec = (reinterpret_cast<uintptr_t>(C) % 16 == 0) && ((size_t)ldc * es) % 16 == 0;
   dim3 grid((unsigned)(M / kBM), (unsigned)(N / BN), (unsigned)((nkb + per - 1) / per));
-  k_gemm_bf16<BN, OUT><<<grid, kGemmThreads, shm, st>>>(A, lda, B, ldb, C, ldc, bias, K, per * kBK, err);
+  k_gemm_tma<BN, OUT><<<grid, kGemmThreads, shm, st>>>(ma, mb, C, ldc, bias, K, per * kBK, vec, err);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(APHID_UNET_ERR_CUDA, std::string("gemm launch: ") + cudaGetErrorString(e));
   return APHID_UNET_OK;

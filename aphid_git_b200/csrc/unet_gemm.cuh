@@ -4,21 +4,15 @@
 //   C[M x N] (op)= A[M x K] B[N x K]^T      A, B: BF16, K contiguous (K-major)
 //                                           accumulation: FP32 in tensor memory
 //
-// One CTA of 128 threads computes a 128 x BN tile.  K is consumed in blocks
-// of 64: all threads copy the A and B blocks into shared memory (cp.async,
-// two buffers) in the canonical K-major, unswizzled core-matrix layout
-// (8 rows x 16 bytes per core matrix); one thread issues four
-// tcgen05.mma.kind::f16 (K = 16 each) per block and commits them to an
-// mbarrier, whose completion frees the buffer for the block after next.
-// The accumulator lives in tensor memory (lane = row, column = n); the
-// epilogue reads it with tcgen05.ld (each warp its 32 lanes) and applies one
-// of the output operations below.  Every wait is bounded: a wait that gives
-// up sets an error flag, and the kernel still drains its own copies and
+// One CTA of 128 threads computes a 128 x BN tile (k_gemm_tma below: TMA
+// producer, single-thread MMA issuer, deep shared-memory ring).  Every wait
+// is bounded: a wait that gives up sets an error flag, and the kernel still
 // frees its tensor memory before it returns.
 //
 // Requirements (checked by the host): M % 128 == 0, N % BN == 0,
 // K % 64 == 0, lda, ldb multiples of 8 elements, 16-byte aligned bases.
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -37,14 +31,6 @@ enum GemmOut {
 };
 
 __device__ __forceinline__ uint32_t gsm(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// shared-memory matrix descriptor, K-major, no swizzle (layout type 0):
-// start address, LBO (between the two K halves of one MMA), SBO (between
-// 8-row groups), descriptor version 1, all in 16-byte units
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
-}
 
 // instruction descriptor of tcgen05.mma.kind::f16: FP32 accumulator, BF16 A
 // and B, both K-major, shape M x N
@@ -67,37 +53,71 @@ __device__ __forceinline__ bool g_mbar_wait(uint32_t bar, uint32_t phase) {
   }
   return false;
 }
-__device__ __forceinline__ void cp16(uint32_t dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// A: 128 x 64 block, B: BN x 64 block; element (r, k) at
-// (k / 8) * (rows * 16) + (r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2
+// ------------------------------------------------------------------------
+// k_gemm_tma: the contraction fed by the tensor-memory accelerator through
+// a deep shared-memory ring.  (A first version copied each 64-wide K block
+// with cp.async by all threads behind a block-wide barrier; the tensor cores
+// idled through every copy, under 1% of their time busy.)  Here:
+//   warp 0, one lane: producer -- for each K block, waits for its ring slot
+//     to be released, then issues two TMA tile loads (A: 128 x 64, B: BN x
+//     64, BF16, 128-byte swizzle) that complete on the slot's "full"
+//     mbarrier;
+//   warp 1, one lane: MMA issuer -- waits for "full", issues four
+//     tcgen05.mma (K = 16 each) on the swizzled tiles and commits them to
+//     the slot's "empty" mbarrier, which releases the slot to the producer;
+//     after the last block it commits once more to "done";
+//   all four warps: epilogue -- wait for "done", read the accumulator from
+//   tensor memory (warp w: lanes 32w..32w+31) and apply the output
+//   operation, with 16-byte stores where the output rows allow them.
+// Shared-memory tiles use the canonical K-major 128-byte-swizzle layout
+// (8-row, 1024-byte atoms; the K = 16 slices of a block start 32 bytes
+// apart inside each 128-byte row), which is what a TMA box with a 128-byte
+// inner extent and CU_TENSOR_MAP_SWIZZLE_128B writes.  No multicast: every
+// load is this CTA's own.  Every wait is bounded and reports through err.
 template <int BN>
-struct GemmShm {
+struct TmaShm {
   static constexpr uint32_t a_bytes = kBM * kBK * 2, b_bytes = BN * kBK * 2;
   static constexpr uint32_t stage = a_bytes + b_bytes;
-  static constexpr size_t bytes = 2 * (size_t)stage + 64;  // + mbarriers, tmem address
+  static constexpr int stages = (int)((196u * 1024u) / stage) < 8 ? (int)((196u * 1024u) / stage) : 8;
+  static constexpr size_t bytes = 1024 + (size_t)stages * stage + 256;  // alignment slack, ring, barriers
 };
+
+// shared-memory descriptor of a K-major tile in the 128-byte-swizzle layout:
+// start address, LBO 16 bytes (unused for swizzled K-major), SBO 1024 bytes
+// (between 8-row atoms), descriptor version 1, layout type 2 (128B swizzle)
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+__device__ __forceinline__ void g_mbar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void g_tma_load2(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          dst),
+      "l"((unsigned long long)map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
 
 template <int BN, int OUT>
 __global__ void __launch_bounds__(kGemmThreads, 1)
-    k_gemm_bf16(const __nv_bfloat16 *__restrict__ A, int lda, const __nv_bfloat16 *__restrict__ B, int ldb,
-                void *C, int ldc, const float *__restrict__ bias, int K, int kchunk, int *err) {
+    k_gemm_tma(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, void *C, int ldc,
+               const float *__restrict__ bias, int K, int kchunk, int vec_out, int *err) {
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "N tile");
-  using SH = GemmShm<BN>;
+  using SH = TmaShm<BN>;
+  constexpr int S = SH::stages;
+  static_assert(S >= 2, "ring");
   constexpr uint32_t kCols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
-  extern __shared__ __align__(128) unsigned char gs[];
-  uint64_t *bars = reinterpret_cast<uint64_t *>(gs + 2 * SH::stage);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(gs + 2 * SH::stage + 16);
-  const int tid = threadIdx.x, warp = tid >> 5;
+  extern __shared__ __align__(1024) unsigned char gs_raw[];
+  // the ring starts on a 1024-byte boundary (the swizzle atom)
+  unsigned char *gs = gs_raw + ((1024u - (gsm(gs_raw) & 1023u)) & 1023u);
+  uint64_t *full = reinterpret_cast<uint64_t *>(gs + S * SH::stage);
+  uint64_t *empty = full + S;
+  uint64_t *done = empty + S;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
-  // split-K: this CTA's range of K
   const int kb0 = blockIdx.z * kchunk, kb1 = min(K, kb0 + kchunk);
   const int nkb = (kb1 - kb0) / kBK;
 
@@ -107,57 +127,43 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  if (tid == 0) {
-    g_mbar_init(gsm(&bars[0]));
-    g_mbar_init(gsm(&bars[1]));
+  if (tid == 32) {
+    for (int q = 0; q < S; q++) {
+      g_mbar_init(gsm(&full[q]));
+      g_mbar_init(gsm(&empty[q]));
+    }
+    g_mbar_init(gsm(done));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tslot;
-
-  auto load = [&](int s, int kb) {  // block kb into buffer s
-    unsigned char *base = gs + s * SH::stage;
-    const int k = kb0 + kb * kBK;
-    for (int c = tid; c < kBM * 8; c += kGemmThreads) {
-      const int r = c >> 3, kc = c & 7;
-      cp16(gsm(base + kc * (kBM * 16) + (r >> 3) * 128 + (r & 7) * 16), A + (size_t)(m0 + r) * lda + k + kc * 8);
-    }
-    for (int c = tid; c < BN * 8; c += kGemmThreads) {
-      const int r = c >> 3, kc = c & 7;
-      cp16(gsm(base + SH::a_bytes + kc * (BN * 16) + (r >> 3) * 128 + (r & 7) * 16),
-           B + (size_t)(n0 + r) * ldb + k + kc * 8);
-    }
-    cp_commit();
-  };
-
-  uint32_t phase[2] = {0, 0};
   bool ok = true;
-  constexpr uint32_t idesc = idesc_bf16(kBM, BN);
-  if (nkb > 0) load(0, 0);
-  for (int kb = 0; kb < nkb; kb++) {
-    const int s = kb & 1;
-    if (kb + 1 < nkb) {
-      if (kb >= 1) {  // buffer s^1 was read by the MMAs of block kb-1
-        ok = g_mbar_wait(gsm(&bars[s ^ 1]), phase[s ^ 1]) && ok;
-        phase[s ^ 1] ^= 1u;
-      }
-      load(s ^ 1, kb + 1);
-      cp_wait<1>();
-    } else {
-      cp_wait<0>();
+
+  if (warp == 0 && lane == 0 && nkb > 0) {
+    // producer
+    for (int kb = 0; kb < nkb; kb++) {
+      const int s = kb % S;
+      if (kb >= S) ok = g_mbar_wait(gsm(&empty[s]), (uint32_t)((kb / S - 1) & 1)) && ok;
+      const uint32_t a = gsm(gs + s * SH::stage), fb = gsm(&full[s]);
+      g_mbar_expect(fb, SH::stage);
+      const int k = kb0 + kb * kBK;
+      g_tma_load2(a, &mapA, k, m0, fb);
+      g_tma_load2(a + SH::a_bytes, &mapB, k, n0, fb);
     }
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // cp.async data -> tensor-core reads
-    __syncthreads();
-    if (tid == 0) {
+  } else if (warp == 1 && lane == 0 && nkb > 0) {
+    // MMA issuer
+    constexpr uint32_t idesc = idesc_bf16(kBM, BN);
+    for (int kb = 0; kb < nkb; kb++) {
+      const int s = kb % S;
+      ok = g_mbar_wait(gsm(&full[s]), (uint32_t)((kb / S) & 1)) && ok;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       const uint32_t a = gsm(gs + s * SH::stage), b = a + SH::a_bytes;
 #pragma unroll
       for (int kk = 0; kk < kBK / 16; kk++) {
-        // K = 16: the two 8-element halves are core matrices 2kk and 2kk+1
-        const uint64_t da = smem_desc(a + 2 * kk * (kBM * 16), kBM * 16, 128);
-        const uint64_t db = smem_desc(b + 2 * kk * (BN * 16), BN * 16, 128);
+        const uint64_t da = smem_desc_sw128(a + 32u * kk), db = smem_desc_sw128(b + 32u * kk);
         const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -166,25 +172,77 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                       gsm(&bars[s]))
+                       gsm(&empty[s]))
                    : "memory");
     }
-    __syncthreads();
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(gsm(done))
+                 : "memory");
   }
-  // the last commit covers every MMA issued before it
-  if (nkb > 0) {
-    const int s = (nkb - 1) & 1;
-    ok = g_mbar_wait(gsm(&bars[s]), phase[s]) && ok;
-    if (nkb >= 2) {  // the other buffer's last commit (block nkb-2) is complete too; consume its phase
-      ok = g_mbar_wait(gsm(&bars[s ^ 1]), phase[s ^ 1]) && ok;
-    }
-  }
+  __syncwarp();
+  if (nkb > 0) ok = g_mbar_wait(gsm(done), 0u) && ok;
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (!ok && err) atomicExch(err, 1);
 
   // epilogue: warp w holds rows 32w .. 32w+31 (tensor-memory lanes)
-  const int row = m0 + warp * 32 + (tid & 31);
+  const int row = m0 + warp * 32 + lane;
   const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  if (OUT != OUT_F32_ATOMIC && BN >= 32 && vec_out) {
+    // wide rows: each warp turns its 32 x 32 blocks around in shared memory
+    // (the ring is free now) so that consecutive lanes store consecutive
+    // 16-byte pieces of one row, instead of each lane writing its own row
+    float *stg = reinterpret_cast<float *>(gs) + warp * (32 * 36);
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+#pragma unroll
+      for (int h = 0; h < 32; h += 8) {
+        uint32_t v[8];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+            : "r"(lane_base + (uint32_t)(c0 + h)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        float x[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          x[q] = nkb == 0 ? 0.f : __uint_as_float(v[q]);
+          if (bias) x[q] += __ldg(bias + n0 + c0 + h + q);
+          if (OUT == OUT_BF16_RELU) x[q] = fmaxf(x[q], 0.f);
+        }
+        float4 *d = reinterpret_cast<float4 *>(stg + lane * 36 + h);
+        d[0] = make_float4(x[0], x[1], x[2], x[3]);
+        d[1] = make_float4(x[4], x[5], x[6], x[7]);
+      }
+      __syncwarp();
+      if (OUT == OUT_F32) {  // 8 lanes per row, 4 rows per step
+#pragma unroll
+        for (int rr = 0; rr < 32; rr += 4) {
+          const int r = rr + (lane >> 3), cq = (lane & 7) * 4;
+          const float4 val = *reinterpret_cast<const float4 *>(stg + r * 36 + cq);
+          *reinterpret_cast<float4 *>(reinterpret_cast<float *>(C) + (size_t)(m0 + warp * 32 + r) * ldc + n0 + c0 +
+                                      cq) = val;
+        }
+      } else {  // BF16: 4 lanes per row, 8 rows per step
+#pragma unroll
+        for (int rr = 0; rr < 32; rr += 8) {
+          const int r = rr + (lane >> 2), cq = (lane & 3) * 8;
+          const float4 a = *reinterpret_cast<const float4 *>(stg + r * 36 + cq);
+          const float4 b = *reinterpret_cast<const float4 *>(stg + r * 36 + cq + 4);
+          uint4 u;
+          u.x = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.x)) |
+                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.y)) << 16);
+          u.y = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.z)) |
+                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a.w)) << 16);
+          u.z = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b.x)) |
+                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b.y)) << 16);
+          u.w = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b.z)) |
+                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b.w)) << 16);
+          *reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(C) + (size_t)(m0 + warp * 32 + r) * ldc + n0 +
+                                     c0 + cq) = u;
+        }
+      }
+      __syncwarp();
+    }
+  } else {
 #pragma unroll 1
   for (int c0 = 0; c0 < BN; c0 += 8) {
     uint32_t v[8];
@@ -193,25 +251,52 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
         : "r"(lane_base + (uint32_t)c0));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    if (nkb == 0) {
+    float x[8];
 #pragma unroll
-      for (int q = 0; q < 8; q++) v[q] = 0u;
+    for (int q = 0; q < 8; q++) x[q] = nkb == 0 ? 0.f : __uint_as_float(v[q]);
+    const int n = n0 + c0;
+    if (OUT == OUT_F32_ATOMIC) {
+      float *cr = reinterpret_cast<float *>(C) + (size_t)row * ldc + n;
+#pragma unroll
+      for (int q = 0; q < 8; q++) atomicAdd(cr + q, x[q]);
+      continue;
     }
+    if (bias) {
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const int n = n0 + c0 + q;
-      float x = __uint_as_float(v[q]);
-      if (OUT == OUT_F32_ATOMIC) {
-        atomicAdd(reinterpret_cast<float *>(C) + (size_t)row * ldc + n, x);
-        continue;
+      for (int q = 0; q < 8; q++) x[q] += __ldg(bias + n + q);
+    }
+    if (OUT == OUT_BF16_RELU) {
+#pragma unroll
+      for (int q = 0; q < 8; q++) x[q] = fmaxf(x[q], 0.f);
+    }
+    if (OUT == OUT_F32) {
+      float *cr = reinterpret_cast<float *>(C) + (size_t)row * ldc + n;
+      if (vec_out) {
+        reinterpret_cast<float4 *>(cr)[0] = make_float4(x[0], x[1], x[2], x[3]);
+        reinterpret_cast<float4 *>(cr)[1] = make_float4(x[4], x[5], x[6], x[7]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; q++) cr[q] = x[q];
       }
-      if (bias) x += __ldg(bias + n);
-      if (OUT == OUT_BF16_RELU) x = fmaxf(x, 0.f);
-      if (OUT == OUT_F32)
-        reinterpret_cast<float *>(C)[(size_t)row * ldc + n] = x;
-      else
-        reinterpret_cast<__nv_bfloat16 *>(C)[(size_t)row * ldc + n] = __float2bfloat16_rn(x);
+    } else {
+      __nv_bfloat16 *cr = reinterpret_cast<__nv_bfloat16 *>(C) + (size_t)row * ldc + n;
+      if (vec_out) {
+        uint4 u;
+        u.x = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[0])) |
+              ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[1])) << 16);
+        u.y = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[2])) |
+              ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[3])) << 16);
+        u.z = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[4])) |
+              ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[5])) << 16);
+        u.w = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[6])) |
+              ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x[7])) << 16);
+        *reinterpret_cast<uint4 *>(cr) = u;
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; q++) cr[q] = __float2bfloat16_rn(x[q]);
+      }
     }
+  }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
