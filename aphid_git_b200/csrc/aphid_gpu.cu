@@ -206,7 +206,9 @@ int ensure_work(aphid_ctx *ctx) {
   CK(cudaMalloc(&ctx->d_sc, sizeof(Scal64)));
   CK(cudaMalloc(&ctx->d_part, (size_t)slots * 3 * sizeof(double)));
   CK(cudaMalloc(&ctx->d_cnt, 16 * sizeof(unsigned)));
-  CK(cudaMemset(ctx->d_cnt, 0, 16 * sizeof(unsigned)));
+  // stream-ordered: the context stream is non-blocking, so work on it does not
+  // wait for the legacy stream that a plain cudaMemset/cudaMemcpy would use
+  CK(cudaMemsetAsync(ctx->d_cnt, 0, 16 * sizeof(unsigned), ctx->stream));
   CK(cudaMalloc(&ctx->d_out, 8 * sizeof(double)));
   return APHID_OK;
 }
@@ -400,7 +402,8 @@ int aphid_gpu_set_mesh(aphid_ctx *ctx, int nx, int ny, int nz, const double *dx,
     all.insert(all.end(), one.begin(), one.end());
   }
   CK(cudaMalloc(&ctx->d_tab, all.size() * sizeof(double)));
-  CK(cudaMemcpy(ctx->d_tab, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(ctx->d_tab, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   GridDev g{};
   for (int a = 0; a < 3; a++) {
     const int m = dims[a];
@@ -909,8 +912,9 @@ int plane_tiles(aphid_ctx *ctx, int kz, int ts) {
   cudaFree(ctx->sw_work);
   ctx->sw_work = nullptr;
   CK(cudaMalloc(&ctx->sw_work, (2 + T) * sizeof(int)));
-  CK(cudaMemset(ctx->sw_work, 0, 2 * sizeof(int)));
-  CK(cudaMemcpy(ctx->sw_work + 2, order.data(), T * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemsetAsync(ctx->sw_work, 0, 2 * sizeof(int), ctx->stream));
+  CK(cudaMemcpyAsync(ctx->sw_work + 2, order.data(), T * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   ctx->ptiles = tp;
   return APHID_OK;
 }
@@ -973,7 +977,7 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     CK(cudaMalloc(&ctx->sw_part, (size_t)nsys * ctx->sw_slots * kParts * sizeof(double)));
     // the counters, then the active-system list of the fused passes (k_sw_active)
     CK(cudaMalloc(&ctx->sw_cnt, ((size_t)CNT_KINDS * nsys + 1 + nsys) * sizeof(unsigned)));
-    CK(cudaMemset(ctx->sw_cnt, 0, (size_t)CNT_KINDS * nsys * sizeof(unsigned)));
+    CK(cudaMemsetAsync(ctx->sw_cnt, 0, (size_t)CNT_KINDS * nsys * sizeof(unsigned), ctx->stream));
     if (!ctx->sw_ndone) CK(cudaMalloc(&ctx->sw_ndone, sizeof(int)));
     ctx->sw_nsys = nsys;
   }
@@ -987,7 +991,7 @@ int sweep_alloc(aphid_ctx *ctx, int nsys, bool mixed) {
     }
     ctx->sw_ring = ring;
     // pads and components that do not exist stay zero for good
-    CK(cudaMemset(ctx->sw_f32, 0, (6 + ring) * v32 * sizeof(float2)));
+    CK(cudaMemsetAsync(ctx->sw_f32, 0, (6 + ring) * v32 * sizeof(float2), ctx->stream));
     if (!ctx->sw_ax32) {
       CK(cudaMalloc(&ctx->sw_ax32, 2 * (size_t)(ctx->nx + ctx->ny + ctx->nz) * sizeof(float4)));
       const int nmax = std::max(ctx->nx, std::max(ctx->ny, ctx->nz));

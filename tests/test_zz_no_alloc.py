@@ -110,6 +110,9 @@ def test_noalloc_deep_slabs_at_the_node_limit():
         out_new = torch.full_like(x_d, float("nan"))
         eps_ref = torch.zeros(2, dtype=torch.float64, device=dev)
         eps_new = torch.full((2,), float("nan"), dtype=torch.float64, device=dev)
+        # the context path runs on its own non-blocking stream: torch's fills
+        # of the inputs and of eps_ref must have landed before it starts
+        torch.cuda.synchronize()
         s.inprod_dev(k2_d.data_ptr(), x_d.data_ptr(), out_ref.data_ptr(), eps_ref.data_ptr())
         torch.cuda.synchronize()
         rc = inprod_eps_noalloc(*dims, [t.data_ptr() for t in spacing], k2_d.data_ptr(), x_d.data_ptr(),
