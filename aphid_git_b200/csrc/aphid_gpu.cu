@@ -1240,6 +1240,28 @@ struct Tuned {
   int kz = 0, cfg = 0, ts = 0;
 };
 
+// The slab depths the tuner times on a mesh of nz z-nodes: one per slab
+// count tk = ceil(nz / c) for c in 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128,
+// 192 and nz, each evened out to ceil(nz / tk), which leaves the last slab
+// of the deep candidates nearly full (193 z-nodes at depth 32 end in a
+// one-plane slab that costs a whole pipeline fill; at depth 28 the seven
+// slabs are 28 x 6 + 25).  Deep slabs serve the complex128 pass,
+// whose pipeline fill per work item is its largest overhead: on the
+// 257 x 257 x 193 seafloor mesh it still gained 3% from depth 24 to 32.
+std::vector<int> tune_depths(int nz) {
+  std::vector<int> out;
+  int last_tk = -1;
+  for (int c : {4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, nz}) {
+    if (c > nz) c = nz;
+    const int tk = (nz + c - 1) / c;
+    const int kz = (nz + tk - 1) / tk;
+    if (kz < kMinKz || tk == last_tk) continue;  // too shallow, or the same slabs as the previous depth
+    last_tk = tk;
+    out.push_back(kz);
+  }
+  return out;
+}
+
 
 std::mutex &tune_mutex() {
   static std::mutex m;
@@ -1333,15 +1355,10 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
     CK(cudaEventCreate(&own.e[1]));
     cudaEvent_t *tev = own.e;
     float best_ms = 0.f;
-    const int cand[] = {4, 6, 8, 12, 16, 24, 32};
+    const std::vector<int> cand = tune_depths(ctx->nz);
     for (int ts = 0; ts < kTileShapes; ts++)
     for (int cfg = 0; cfg < (fused ? 1 : 2); cfg++) {
-      int last_tk = -1;
       for (int c : cand) {
-        if (c > ctx->nz) break;
-        const int tk = (ctx->nz + c - 1) / c;
-        if (tk == last_tk) continue;  // same slabs as the previous candidate
-        last_tk = tk;
         if ((rc = plane_tiles(ctx, c, ts))) return rc;
         ctx->pass_cfg = cfg;
         SweepDev D = sweep_dev(ctx, nsys);
