@@ -544,19 +544,16 @@ def main():
     if not args.no_fused64:
         try:
             # the first FUSED64 sweep of a batch size tunes the complex128
-            # pass; where a sweep is short, that tuning would dominate the
-            # leg, so one untimed sweep runs first (on long sweeps it is a
-            # second or so of a half-minute leg, and is kept)
-            warm64 = ms / args.steps < 5000.0
-            if warm64:
-                sweep("fused64")
+            # pass (24 timed configurations, about 3 s on seafloor256): one
+            # untimed sweep runs first, so that the leg times the solve alone
+            sweep("fused64")
             ms_f, inf_f = timed(stream, dev, lambda: sweep("fused64"), 1, barrier, world)
             fi = inf_f[-1] or [{"inner_iters": 0, "status_name": "none"}]
             extra["fused64_sweep"] = {"time_s": ms_f * 1e-3, "iters": [i["inner_iters"] for i in fi],
                                       "status": sorted({i["status_name"] for i in fi}),
                                       "note": "batched complex128 pass (k_sw_pass64) for every system, in "
                                               "as many chunks as device memory holds",
-                                      "tuned_before_timing": warm64}
+                                      "tuned_before_timing": True}
             extra["speedup_vs_fused64_sweep"] = ms_f / (ms / args.steps)
         except Exception as e:  # a comparison leg: report, keep the line
             extra["fused64_sweep"] = {"error": str(e)}
