@@ -1354,31 +1354,40 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
     CK(cudaEventCreate(&own.e[0]));
     CK(cudaEventCreate(&own.e[1]));
     cudaEvent_t *tev = own.e;
+    // time one configuration: 5 passes after 2 untimed ones (ms for the 5)
+    auto time_cfg = [&](const Tuned &t, float &ms) -> int {
+      int rc1;
+      if ((rc1 = plane_tiles(ctx, t.kz, t.ts))) return rc1;
+      ctx->pass_cfg = t.cfg;
+      SweepDev D = sweep_dev(ctx, nsys);
+      D.tmix = 0.f;
+      auto pass = [&]() {
+        if (fused)
+          launch_pass64(ctx, D, true);
+        else
+          launch_pass(ctx, D, true);
+      };
+      for (int r = 0; r < 2; r++) pass();
+      CK(cudaEventRecord(tev[0], ctx->stream));
+      for (int r = 0; r < 5; r++) pass();
+      CK(cudaEventRecord(tev[1], ctx->stream));
+      CK(cudaEventSynchronize(tev[1]));
+      CK(cudaGetLastError());
+      CK(cudaEventElapsedTime(&ms, tev[0], tev[1]));
+      return APHID_OK;
+    };
+    std::vector<std::pair<Tuned, float>> timed;
     float best_ms = 0.f;
     const std::vector<int> cand = tune_depths(ctx->nz);
     for (int ts = 0; ts < kTileShapes; ts++)
     for (int cfg = 0; cfg < (fused ? 1 : 2); cfg++) {
       for (int c : cand) {
-        if ((rc = plane_tiles(ctx, c, ts))) return rc;
-        ctx->pass_cfg = cfg;
-        SweepDev D = sweep_dev(ctx, nsys);
-        D.tmix = 0.f;
-        auto pass = [&]() {
-          if (fused)
-            launch_pass64(ctx, D, true);
-          else
-            launch_pass(ctx, D, true);
-        };
-        for (int r = 0; r < 2; r++) pass();
-        CK(cudaEventRecord(tev[0], ctx->stream));
-        for (int r = 0; r < 5; r++) pass();
-        CK(cudaEventRecord(tev[1], ctx->stream));
-        CK(cudaEventSynchronize(tev[1]));
-        CK(cudaGetLastError());
+        const Tuned t{c, cfg, ts};
         float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, tev[0], tev[1]));
+        if ((rc = time_cfg(t, ms))) return rc;
+        timed.push_back({t, ms});
         if (!best.kz || ms < best_ms) {
-          best = Tuned{c, cfg, ts};
+          best = t;
           best_ms = ms;
         }
         if (ctx->verbose)
@@ -1386,6 +1395,28 @@ int tune_kz(aphid_ctx *ctx, int nsys, bool fused = false) {
                        fused ? " (c128)" : "");
       }
     }
+    // Configurations within 2% of the fastest are timed twice more and
+    // judged by their best of three: one five-pass timing under the power
+    // cap varies by a few tenths of a percent, as much as neighbouring
+    // depths differ, and the choice fixes the summation order of the whole
+    // solve.
+    const float near = best_ms * 1.02f;
+    for (auto &tm : timed) {
+      if (tm.second > near) continue;
+      for (int r = 0; r < 2; r++) {
+        float ms = 0.f;
+        if ((rc = time_cfg(tm.first, ms))) return rc;
+        tm.second = std::min(tm.second, ms);
+      }
+      if (ctx->verbose)
+        std::fprintf(stderr, "aphid_gpu: tune ts=%d kz=%d cfg=%d best of 3 %.3f ms/pass%s\n", tm.first.ts,
+                     tm.first.kz, tm.first.cfg, tm.second / 5, fused ? " (c128)" : "");
+    }
+    for (const auto &tm : timed)
+      if (tm.second < best_ms) {
+        best = tm.first;
+        best_ms = tm.second;
+      }
     int kerr = 0;
     CK(cudaMemcpy(&kerr, ctx->sw_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (kerr) return fail(ctx, APHID_ERR_CUDA, "tuner: a tensor-copy wait in the pass timed out");
