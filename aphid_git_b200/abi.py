@@ -415,8 +415,10 @@ class Solver:
         return y
 
     def sweep_plane_kz(self):
-        """z-planes per work item of the complex64 pass in use (the
-        autotuner's choice unless plane_kz was fixed); 0 before a mixed sweep."""
+        """z-planes per work item of the fused pass that ran last (the
+        autotuner's choice unless plane_kz was fixed): the complex128 pass's
+        after an escalating AUTO sweep or a FUSED64 sweep, else the complex64
+        pass's; 0 before a mixed sweep."""
         return int(self.lib.aphid_gpu_sweep_plane_kz(self._h))
 
     def sweep_pass_config(self):

@@ -312,9 +312,10 @@ int aphid_gpu_sweep_group(int njob, const aphid_group_job *jobs,
 int aphid_gpu_sweep_receivers(aphid_ctx *ctx, int nrec, const int *rec_ijk,
                               aphid_z *E, aphid_z *H);
 
-/* z-planes per work item of the complex64 pass in use (the autotuner's
- * choice unless aphid_opts.plane_kz fixed it); 0 before the first mixed
- * sweep. */
+/* z-planes per work item of the fused pass that ran last (the autotuner's
+ * choice unless aphid_opts.plane_kz fixed it): the complex128 pass's after
+ * an AUTO sweep that escalated systems or a FUSED64 sweep, else the
+ * complex64 pass's; 0 before the first mixed sweep. */
 int aphid_gpu_sweep_plane_kz(aphid_ctx *ctx);
 
 /* Pipeline configuration of the complex64 pass in use: 0 = two load stages
