@@ -446,6 +446,45 @@ def test_tile_shapes_agree(tmp_path, monkeypatch, precision):
         assert relerr(a, b) < 1e-7
 
 
+@pytest.mark.parametrize("mode,cfg", [("R", 0), ("C", 1)])
+def test_lone_last_tile_column_matches_oracle(tmp_path, monkeypatch, mode, cfg):
+    """A mesh of 33 x 17 x 14 nodes: 33 = 32 + 1 = 2 x 16 + 1, so in both tile
+    shapes the last tile column holds one live node column (as on the
+    257-node benchmark meshes).  Both shapes, forced through the tune cache:
+    the pass's operator against the oracle's K row by row, and converged
+    sweeps that agree with each other."""
+    sms, name_hash = _device_identity()
+    xn, yn, zn, sig, epsr = small_model(seed=17, dims=(33, 17, 14), nair=3)
+    sig[:, :, 3:5] = 3.3
+    src = [[("+X", 16, 8, 4)], [("+Y", 30, 3, 5)]]  # the second one near the last node column
+    w = [2 * np.pi * f for f in (0.3, 30.0)]
+    kind = 0 if mode == "R" else 1
+    out = []
+    for ts in (0, 1):
+        cache = tmp_path / ("lone%d.txt" % ts)
+        cache.write_text("33 17 14 %d %d %d %d 6 %d %d\n" % (2 + ts, kind, sms, name_hash, cfg, ts))
+        monkeypatch.setenv("APHID_TUNE_CACHE", str(cache))
+        with Solver(graph_iters=8) as s:
+            s.set_nodes(xn, yn, zn)
+            s.set_model(mode, sig, None if mode == "R" else epsr)
+            X, inf = s.sweep(w + w[:ts], src, [0, 1, 0][:2 + ts], precision="mixed", target=1e-9)
+            assert s.sweep_tile_shape() == ts and s.sweep_plane_kz() == 6 and s.sweep_pass_config() == cfg
+            assert all(i["status_name"] == "converged" for i in inf), inf
+            g = O.Grid(xn, yn, zn)
+            k2 = O.gen_k2(g, O.sigma_hat(mode, w[0], sig_re=sig, eps_rel=None if mode == "R" else epsr), w[0])
+            rng = np.random.default_rng(9)
+            x = rng.standard_normal(g.n) + 1j * rng.standard_normal(g.n)
+            y64 = O.inprod(g, k2, x)
+            y = s.sweep_apply(x)  # system 0: w[0]
+            floor = 1e-3 * np.sqrt(np.mean(np.abs(y64) ** 2))
+            assert relerr(y, y64) < 1e-6
+            assert np.max(np.abs(y - y64) / (np.abs(y64) + floor)) < 1e-5
+            out.append(X[:2])
+        assert len(cache.read_text().splitlines()) == 1  # the record was used, not retuned
+    for a, b in zip(*out):
+        assert relerr(a, b) < 1e-7
+
+
 @pytest.mark.parametrize("precision,tol_norm,tol_row", [("mixed", 1e-6, 1e-5), ("fused64", 1e-13, 1e-11)])
 @pytest.mark.parametrize("mode", ["R", "C"])
 def test_pass_operator_matches_oracle_row_by_row(solver, mode, precision, tol_norm, tol_row):
